@@ -1,0 +1,322 @@
+"""GLST energy+force throughput on B200 (one JSON line on rank 0).
+
+Workload (N=1): 10,000 TIP3P-like waters (30,000 atoms), cubic box L = 66.9 A,
+cutoff 10 A, splitting alpha = 0.31 1/A (tol = erfc(3.1)/10), the default
+cubature order; mixed precision.  A step = one energy+force solve of that
+system (glst_compute: assignment, near field, structure factors, shell sums,
+long-range gather, combine).  Metric: atom-evals/s = atoms solved / second.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+For N > 1 (torchrun, one rank per GPU) every rank solves its own copy of the
+system (independent systems, no collective on the data path): weak scaling,
+value = all ranks' atoms / max-over-ranks time.
+--impl reference times the FP64 CPU restatement of the reference's GLST sum
+(the reference ships no CPU implementation; its own code is CUDA) on the
+host's cores, on a node subset of the same workload, extrapolated by K.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+import __graft_entry__  # noqa: E402
+
+METRIC = "atom-evals/s at <=1e-5 force RMS err vs FP64"
+UNIT = "atom-evals/s"
+WORKLOAD = "water10k"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl" if args.impl == "ours" else "gloo",
+                                timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def cpu_baseline_run(sysd, K_sample_div=32):
+    """FP64 oracle on the host: full near field + a node subset of the far
+    field, extrapolated linearly in the number of nodes."""
+    from oracle import oracle, planner
+    g = __graft_entry__.load_package()
+    store = planner.TDesignStore(g.TDESIGN_STORE)
+    x, y, z, q = sysd["x"], sysd["y"], sysd["z"], sysd["q"]
+    p = planner.make_plan(len(x), sysd["tol"], sysd["box"], sysd["rcut"], store)
+    ks = max(1, p.K // K_sample_div)
+    t0 = time.perf_counter()
+    oracle.glst(x, y, z, q, p, far=False, sr=True)
+    t_sr = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.glst(x, y, z, q, p, k0=0, k1=ks, far=True, sr=False)
+    t_far = time.perf_counter() - t0
+    t_est = t_sr + t_far * (p.K / ks)
+    return dict(seconds_per_solve=t_est, cores=oracle.num_threads(), K=p.K, K_sample=ks,
+                t_near=t_sr, t_far_sample=t_far)
+
+
+def run_reference(args, world, rank):
+    from glst_b200 import systems
+    if rank != 0:
+        return
+    sysd = systems.config_system(args.workload, seed=0)
+    n = len(sysd["x"])
+    times = []
+    info = None
+    for it in range(args.warmup + args.steps):
+        r = cpu_baseline_run(sysd)
+        if it >= args.warmup:
+            times.append(r["seconds_per_solve"])
+        info = r
+    sec = statistics.mean(times)
+    val = n / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded TIP3P-like water)",
+        "config": {"workload": args.workload, "atoms": n, "nodes": info["K"],
+                   "sample": "all atoms, near field in full, far field on %d of %d nodes, extrapolated in K"
+                             % (info["K_sample"], info["K"])},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": info["cores"], "kind": "port",
+                         "sample": "node subset %d/%d, linear in K" % (info["K_sample"], info["K"])},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local, dist):
+    import torch
+    g = __graft_entry__.load_package()
+    from glst_b200 import systems
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    sysd = systems.config_system(args.workload, seed=0)
+    n = len(sysd["x"])
+    L = sysd["box"][0]
+    f = g.GlstForce(n, sysd["tol"], L, L, L, rcut=sysd["rcut"])
+    inf = f.info()
+    d = [torch.tensor(sysd[k], dtype=torch.float64, device=dev) for k in ("x", "y", "z", "q")]
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    for _ in range(args.warmup):
+        f.calc_ener_force(*d, stream=stream)
+    torch.cuda.synchronize()
+    f.check(stream=stream)
+
+    # per-phase times of one instrumented step (same stream, CUDA events)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(7)]
+    flush.zero_()
+    ev[0].record(stream)
+    f.assign_atoms(*d, stream=stream)
+    ev[1].record(stream)
+    f.calc_sr_ef(stream=stream)
+    ev[2].record(stream)
+    f.calc_sf(stream=stream)
+    ev[3].record(stream)
+    f.sum_rmt_sf(stream=stream)
+    ev[4].record(stream)
+    f.calc_lr_ef(stream=stream)
+    ev[5].record(stream)
+    f.comm_ef(stream=stream)
+    ev[6].record(stream)
+    torch.cuda.synchronize()
+    names = ["assign", "near_field", "structure_factors", "shell_sums", "long_range", "combine"]
+    phases = {nm: ev[i].elapsed_time(ev[i + 1]) for i, nm in enumerate(names)}
+
+    # timed region: K steps, L2 flushed between steps (outside the step events)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    wall0 = time.perf_counter()
+    for i in range(args.steps):
+        flush.zero_()
+        starts[i].record(stream)
+        f.calc_ener_force(*d, stream=stream)
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    clk = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    f.check(stream=stream)
+    value = world * n * args.steps / (total_ms * 1e-3)
+
+    # end to end through the public API from pinned host memory
+    hx = [torch.tensor(sysd[k], dtype=torch.float64).pin_memory() for k in ("x", "y", "z", "q")]
+    ho = [torch.empty(n, dtype=torch.float64).pin_memory() for _ in range(4)]
+    lib = g.load_library()
+
+    def host_step():
+        st = lib.glst_compute_host(f._h, *[t.data_ptr() for t in hx], *[t.data_ptr() for t in ho],
+                                   stream.cuda_stream)
+        if st:
+            raise g.GlstError(st, lib.glst_last_error().decode())
+
+    for _ in range(2):
+        host_step()
+    e_steps = max(3, args.steps // 2)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e_steps):
+        host_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_val = world * n * e_steps / (e2e_ms * 1e-3)
+
+    # roofline of the dominant kernel (SFU-bound phase kernels)
+    sfu_peak, fma_peak = g.measure_pipe_peaks()
+    K = inf.num_nodes
+    dom = max(("structure_factors", "long_range"), key=lambda k: phases[k])
+    pairs = float(n) * K  # (atom, node) phase evaluations per launch
+    achieved_sfu = 2.0 * pairs / (phases[dom] * 1e-3)  # sin + cos per pair
+    roofline = {
+        "bound": "sfu", "kernel": dom, "achieved": achieved_sfu / 1e9, "peak": sfu_peak / 1e9,
+        "unit": "G sincos-results/s", "frac": achieved_sfu / sfu_peak,
+        "peak_source": "measured on this GPU by glst_measure_pipe_peaks (MUFU sin+cos loop)",
+        "traffic": None, "pairs_per_launch": pairs,
+        "fp32_fma_peak_per_s": fma_peak,
+    }
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 phases/sincos + f64 cell-relative/shell/energy",
+        "data": "synthetic (seeded TIP3P-like water, no dataset)",
+        "config": {"workload": args.workload, "atoms": n, "box_A": L, "rcut_A": sysd["rcut"],
+                   "tol": sysd["tol"], "cells": list(inf.ncell), "groups": inf.ngroup, "nodes": K,
+                   "parallelism": "dp%d (independent systems)" % world,
+                   "l2": "flushed (256 MB write) between timed steps"},
+        "clocks": clk,
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 4 * 8 * n, "d2h_bytes_per_step": 4 * 8 * n,
+                "path": "glst_compute_host (pinned host buffers, H2D + solve + D2H per step)"},
+        "gpu_launches": 10 * args.steps,
+        "phases_ms": phases,
+        "roofline": roofline,
+        "wall_s_timed": wall,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline_run(sysd)
+        line["cpu_baseline"] = {"value": n / cb["seconds_per_solve"], "unit": UNIT, "cores": cb["cores"],
+                                "kind": "port",
+                                "sample": "FP64 oracle: near field in full + far field on %d of %d nodes "
+                                          "(%.1f s), extrapolated linearly in K" % (
+                                              cb["K_sample"], cb["K"], cb["t_near"] + cb["t_far_sample"])}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    f.close()
+
+
+def main():
+    args = parse()
+    world, rank, local, dist = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local, dist)
+    finally:
+        if dist:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

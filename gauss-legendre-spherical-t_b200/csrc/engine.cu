@@ -1,0 +1,649 @@
+// Host runtime behind the C-ABI (include/glst_c.h): owns the plan, the device
+// buffers and the launch sequence of one GLST system on one GPU.
+#include <dlfcn.h>
+#include <sys/stat.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "glst_c.h"
+#include "kernels.cuh"
+#include "planner.hpp"
+
+using glst::Plan;
+using glst::PlanError;
+using glst::TDesignStore;
+namespace dev = glst::dev;
+
+// ---------------------------------------------------------------- errors
+static thread_local std::string g_last_error;
+
+static glst_status fail(glst_status s, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return s;
+}
+
+#define CUDA_TRY(call)                                                          \
+  do {                                                                          \
+    cudaError_t e_ = (call);                                                    \
+    if (e_ != cudaSuccess)                                                      \
+      return fail(e_ == cudaErrorMemoryAllocation ? GLST_ERR_OUT_OF_MEMORY      \
+                                                  : GLST_ERR_CUDA,              \
+                  "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),       \
+                  __FILE__, __LINE__);                                          \
+  } while (0)
+
+#define GLST_TRY(expr)            \
+  do {                            \
+    glst_status s_ = (expr);      \
+    if (s_ != GLST_OK) return s_; \
+  } while (0)
+
+// ---------------------------------------------------------------- t-designs
+static std::mutex g_store_mu;
+static std::string g_store_path;  // explicit override
+static std::map<std::string, std::shared_ptr<TDesignStore>> g_stores;
+
+static std::string library_dir() {
+  Dl_info info;
+  if (dladdr(reinterpret_cast<void *>(&library_dir), &info) && info.dli_fname) {
+    std::string p = info.dli_fname;
+    size_t s = p.rfind('/');
+    if (s != std::string::npos) return p.substr(0, s);
+  }
+  return ".";
+}
+
+static bool path_exists(const std::string &p) {
+  struct stat st;
+  return stat(p.c_str(), &st) == 0;
+}
+
+static std::string resolve_store_path() {
+  if (!g_store_path.empty()) return g_store_path;
+  if (const char *e = std::getenv("GLST_TDESIGN_PATH"))
+    if (*e) return e;
+  if (path_exists("SS31-Mar-2016/")) return "SS31-Mar-2016/";
+  return library_dir() + "/data/tdesigns.bin";
+}
+
+static std::shared_ptr<TDesignStore> get_store() {
+  std::lock_guard<std::mutex> lk(g_store_mu);
+  const std::string p = resolve_store_path();
+  auto it = g_stores.find(p);
+  if (it != g_stores.end()) return it->second;
+  auto s = TDesignStore::open(p);
+  g_stores[p] = s;
+  return s;
+}
+
+// ---------------------------------------------------------------- handle
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+struct glst_handle {
+  Plan plan;
+  int device = 0;
+  dev::Grid grid{};
+  uint32_t K = 0;
+  uint32_t nsplit = 1, nodes_per_split = 0;
+  uint32_t sat_nb = 1, sat_stride = 0;
+  size_t sat_smem = 0;
+  uint32_t combine_blocks = 1;
+  bool computed = false;
+  std::vector<DevBuf> bufs;
+  uint64_t bytes = 0;
+  // atoms
+  uint32_t *atom_cell = nullptr, *atom_slot = nullptr, *perm = nullptr;
+  uint32_t *sorted_idx = nullptr, *cell_count = nullptr, *cell_point = nullptr;
+  uint32_t *flags = nullptr;
+  float4 *pk = nullptr;
+  double4 *pd = nullptr;
+  // nodes
+  float4 *node32 = nullptr;
+  double4 *node64 = nullptr;
+  uint32_t *node_radii = nullptr;
+  // far field
+  double2 *S = nullptr;
+  float2 *R = nullptr;
+  double4 *part = nullptr;
+  double4 *sr = nullptr;
+  // outputs
+  double *cfx = nullptr, *cfy = nullptr, *cfz = nullptr, *cen = nullptr;
+  double *ofx = nullptr, *ofy = nullptr, *ofz = nullptr, *oen = nullptr;
+  double *block_energy = nullptr, *energy = nullptr;
+  // host-visible staging for the end-to-end path
+  double *in_host = nullptr;  // device copy of host inputs (4 x natom)
+  // streams/events for the near-field fork
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+};
+
+static glst_status dalloc(glst_handle *h, void **out, size_t bytes) {
+  *out = nullptr;
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(out, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(GLST_ERR_OUT_OF_MEMORY, "cudaMalloc(%zu bytes) failed: %s", bytes,
+                cudaGetErrorString(e));
+  }
+  h->bufs.push_back({*out, bytes});
+  h->bytes += bytes;
+  return GLST_OK;
+}
+
+template <typename T>
+static glst_status dalloc_n(glst_handle *h, T **out, size_t n) {
+  return dalloc(h, reinterpret_cast<void **>(out), n * sizeof(T));
+}
+
+static void release(glst_handle *h) {
+  for (auto &b : h->bufs) cudaFree(b.p);
+  h->bufs.clear();
+  h->bytes = 0;
+  if (h->side) cudaStreamDestroy(h->side);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
+  h->side = nullptr;
+  h->ev_fork = h->ev_join = nullptr;
+}
+
+static glst_status setup(glst_handle *h, uint32_t natom, double tol,
+                         const double box[3], double rcut, int ct_float) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+    cudaGetLastError();
+    return fail(GLST_ERR_NO_DEVICE, "no CUDA capable device found");
+  }
+  CUDA_TRY(cudaGetDevice(&h->device));
+  try {
+    auto store = get_store();
+    h->plan = glst::make_plan(natom, tol, box, rcut, ct_float, *store);
+  } catch (const PlanError &e) {
+    return fail(static_cast<glst_status>(e.status), "%s", e.msg.c_str());
+  } catch (const std::exception &e) {
+    return fail(GLST_ERR_TDESIGN, "planning failed: %s", e.what());
+  }
+  const Plan &p = h->plan;
+  h->grid = dev::Grid{p.n[0], p.n[1], p.n[2], p.ncell, p.cell_dim, p.ct_float};
+  h->K = p.has_far ? p.K() : 0;
+  const size_t N = natom, C = p.ncell, K = h->K;
+
+  // Node arrays.  Nodes and weights are rounded to CT first, as the
+  // reference stores them (src/cubature.cu:138-141).
+  {
+    std::vector<float4> n32(K);
+    std::vector<double4> n64(K);
+    std::vector<uint32_t> radii(K);
+    for (size_t k = 0; k < K; k++) {
+      double kx = p.kx[k], ky = p.ky[k], kz = p.kz[k], w = p.w[k];
+      if (p.ct_float) {
+        kx = (double)(float)kx; ky = (double)(float)ky; kz = (double)(float)kz; w = (double)(float)w;
+      }
+      n64[k] = make_double4(kx, ky, kz, w);
+      n32[k] = make_float4((float)kx, (float)ky, (float)kz, 0.f);
+      const auto &g = p.groups[p.group[k]];
+      radii[k] = (g.r_in & 0xffffu) | (g.r_out << 16);
+    }
+    GLST_TRY(dalloc_n(h, &h->node32, K));
+    GLST_TRY(dalloc_n(h, &h->node64, K));
+    GLST_TRY(dalloc_n(h, &h->node_radii, K));
+    if (K) {
+      CUDA_TRY(cudaMemcpy(h->node32, n32.data(), K * sizeof(float4), cudaMemcpyHostToDevice));
+      CUDA_TRY(cudaMemcpy(h->node64, n64.data(), K * sizeof(double4), cudaMemcpyHostToDevice));
+      CUDA_TRY(cudaMemcpy(h->node_radii, radii.data(), K * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    }
+  }
+  GLST_TRY(dalloc_n(h, &h->atom_cell, N));
+  GLST_TRY(dalloc_n(h, &h->atom_slot, N));
+  GLST_TRY(dalloc_n(h, &h->perm, N));
+  GLST_TRY(dalloc_n(h, &h->sorted_idx, N));
+  GLST_TRY(dalloc_n(h, &h->cell_count, C));
+  GLST_TRY(dalloc_n(h, &h->cell_point, C));
+  GLST_TRY(dalloc_n(h, &h->flags, 4));
+  GLST_TRY(dalloc_n(h, &h->pk, N));
+  GLST_TRY(dalloc_n(h, &h->pd, N));
+  GLST_TRY(dalloc_n(h, &h->sr, N));
+  for (double **o : {&h->cfx, &h->cfy, &h->cfz, &h->cen, &h->ofx, &h->ofy, &h->ofz, &h->oen})
+    GLST_TRY(dalloc_n(h, o, N));
+  h->combine_blocks = (uint32_t)std::max<size_t>(1, (N + dev::kCombineThreads - 1) / dev::kCombineThreads);
+  GLST_TRY(dalloc_n(h, &h->block_energy, h->combine_blocks));
+  GLST_TRY(dalloc_n(h, &h->energy, 1));
+  GLST_TRY(dalloc_n(h, &h->in_host, 4 * N));
+
+  if (K) {
+    // Shared-memory plan of the shell-sum kernel: as many nodes per CTA as
+    // fit (rows of ncell+1 complex doubles), at most 32.
+    int smem_optin = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+    h->sat_stride = (uint32_t)(C + 1);
+    const size_t row = (size_t)h->sat_stride * sizeof(double2);
+    const size_t budget = std::min<size_t>((size_t)smem_optin, 200 * 1024);
+    if (row > budget)
+      return fail(GLST_ERR_SIZE,
+                  "cell grid of %zu cells exceeds the shell-sum shared-memory limit (%zu cells)",
+                  C, budget / sizeof(double2) - 1);
+    h->sat_nb = (uint32_t)std::min<size_t>(32, budget / row);
+    h->sat_smem = row * h->sat_nb;
+    // one process-wide maximum, so handles with different plans coexist
+    CUDA_TRY(cudaFuncSetAttribute(dev::k_shell_sums, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)budget));
+    // Node splits of the long-range gather: enough CTAs to fill the GPU.
+    int nsm = 148;
+    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+    const size_t want = (size_t)nsm * 16;
+    size_t nsplit = (want + C - 1) / C;
+    nsplit = std::max<size_t>(1, std::min<size_t>(nsplit, (K + 1023) / 1024));
+    nsplit = std::min<size_t>(nsplit, 65535);
+    h->nodes_per_split = (uint32_t)((K + nsplit - 1) / nsplit);
+    h->nodes_per_split = ((h->nodes_per_split + dev::kLrTile - 1) / dev::kLrTile) * dev::kLrTile;
+    h->nsplit = (uint32_t)((K + h->nodes_per_split - 1) / h->nodes_per_split);
+    GLST_TRY(dalloc_n(h, &h->S, C * K));
+    GLST_TRY(dalloc_n(h, &h->R, C * K));
+    GLST_TRY(dalloc_n(h, &h->part, (size_t)h->nsplit * N));
+  }
+  CUDA_TRY(cudaFuncSetAttribute(dev::k_sort_pack, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(dev::kSortCap * sizeof(uint32_t))));
+  CUDA_TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+  CUDA_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+  CUDA_TRY(cudaMemset(h->flags, 0, 4 * sizeof(uint32_t)));
+  h->computed = false;
+  return GLST_OK;
+}
+
+// ---------------------------------------------------------------- phases
+static inline cudaStream_t S_(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+static glst_status phase_assign(glst_handle *h, const double *rx, const double *ry,
+                                const double *rz, const double *qc, cudaStream_t st) {
+  const uint32_t N = h->plan.natom, C = h->plan.ncell;
+  if (N && (!rx || !ry || !rz || !qc)) return fail(GLST_ERR_INVALID_ARG, "null input pointer");
+  CUDA_TRY(cudaMemsetAsync(h->cell_count, 0, C * sizeof(uint32_t), st));
+  CUDA_TRY(cudaMemsetAsync(h->flags, 0, 4 * sizeof(uint32_t), st));
+  if (N) {
+    const uint32_t nb = (N + 255) / 256;
+    dev::k_bin<<<nb, 256, 0, st>>>(rx, ry, rz, N, h->grid, h->atom_cell, h->atom_slot, h->cell_count);
+    CUDA_TRY(cudaGetLastError());
+  }
+  dev::k_scan<<<1, 1024, 0, st>>>(h->cell_count, C, h->cell_point, h->flags);
+  CUDA_TRY(cudaGetLastError());
+  if (N) {
+    const uint32_t nb = (N + 255) / 256;
+    dev::k_scatter<<<nb, 256, 0, st>>>(h->atom_cell, h->atom_slot, h->cell_point, N, h->perm);
+    CUDA_TRY(cudaGetLastError());
+    dev::k_sort_pack<<<C, 256, dev::kSortCap * sizeof(uint32_t), st>>>(
+        h->perm, h->cell_count, h->cell_point, h->grid, rx, ry, rz, qc, h->sorted_idx, h->pk, h->pd);
+    CUDA_TRY(cudaGetLastError());
+  }
+  return GLST_OK;
+}
+
+static glst_status phase_sf(glst_handle *h, cudaStream_t st) {
+  if (!h->K || !h->plan.natom) return GLST_OK;
+  const uint32_t per = dev::kSfThreads * dev::kSfNodesPerThread;
+  const uint32_t cg = (h->plan.ncell + dev::kSfCellsPerCta - 1) / dev::kSfCellsPerCta;
+  if (cg > 65535) return fail(GLST_ERR_SIZE, "too many cells for the structure-factor grid");
+  dim3 grid((h->K + per - 1) / per, cg);
+  dev::k_structure_factors<<<grid, dev::kSfThreads, 0, st>>>(h->pk, h->cell_count, h->cell_point, h->grid,
+                                                             h->node32, h->node64, h->K, h->S);
+  CUDA_TRY(cudaGetLastError());
+  return GLST_OK;
+}
+
+static glst_status phase_shell(glst_handle *h, cudaStream_t st) {
+  if (!h->K || !h->plan.natom) return GLST_OK;
+  dev::SatArgs a{h->S, h->node64, h->node_radii, h->K, h->sat_nb, h->sat_stride, h->R};
+  const uint32_t nblk = (h->K + h->sat_nb - 1) / h->sat_nb;
+  dev::k_shell_sums<<<nblk, dev::kSatThreads, h->sat_smem, st>>>(h->grid, a);
+  CUDA_TRY(cudaGetLastError());
+  return GLST_OK;
+}
+
+static glst_status phase_lr(glst_handle *h, cudaStream_t st) {
+  if (!h->K || !h->plan.natom) return GLST_OK;
+  dim3 grid(h->plan.ncell, h->nsplit);
+  dev::k_long_range<<<grid, dev::kLrThreads, 0, st>>>(h->pk, h->cell_count, h->cell_point, h->node32, h->R,
+                                                      h->K, h->nodes_per_split, h->plan.natom, h->part);
+  CUDA_TRY(cudaGetLastError());
+  return GLST_OK;
+}
+
+static glst_status phase_sr(glst_handle *h, cudaStream_t st) {
+  if (!h->plan.natom) return GLST_OK;
+  dev::k_short_range<<<h->plan.ncell, dev::kSrThreads, 0, st>>>(h->pd, h->cell_count, h->cell_point,
+                                                                 h->grid, h->sr);
+  CUDA_TRY(cudaGetLastError());
+  return GLST_OK;
+}
+
+static glst_status phase_combine(glst_handle *h, cudaStream_t st) {
+  const uint32_t N = h->plan.natom;
+  if (N) {
+    dev::k_combine<<<h->combine_blocks, dev::kCombineThreads, 0, st>>>(
+        h->sr, h->part, h->nsplit, h->sorted_idx, N, h->K ? 1 : 0, h->cfx, h->cfy, h->cfz, h->cen,
+        h->ofx, h->ofy, h->ofz, h->oen, h->block_energy);
+    CUDA_TRY(cudaGetLastError());
+    dev::k_energy_total<<<1, 256, 0, st>>>(h->block_energy, h->combine_blocks, h->energy);
+    CUDA_TRY(cudaGetLastError());
+  } else {
+    CUDA_TRY(cudaMemsetAsync(h->energy, 0, sizeof(double), st));
+  }
+  h->computed = true;
+  return GLST_OK;
+}
+
+static glst_status compute_all(glst_handle *h, const double *rx, const double *ry, const double *rz,
+                               const double *qc, cudaStream_t st) {
+  GLST_TRY(phase_assign(h, rx, ry, rz, qc, st));
+  // The near field (FP64 pipe) runs on a side stream, overlapping the far
+  // field (SFU/FP32 pipes) on the same SMs.
+  CUDA_TRY(cudaEventRecord(h->ev_fork, st));
+  CUDA_TRY(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+  GLST_TRY(phase_sr(h, h->side));
+  CUDA_TRY(cudaEventRecord(h->ev_join, h->side));
+  GLST_TRY(phase_sf(h, st));
+  GLST_TRY(phase_shell(h, st));
+  GLST_TRY(phase_lr(h, st));
+  CUDA_TRY(cudaStreamWaitEvent(st, h->ev_join, 0));
+  return phase_combine(h, st);
+}
+
+// ---------------------------------------------------------------- C-ABI
+extern "C" {
+
+const char *glst_last_error(void) { return g_last_error.c_str(); }
+
+const char *glst_status_string(glst_status s) {
+  switch (s) {
+    case GLST_OK: return "ok";
+    case GLST_ERR_INVALID_ARG: return "invalid argument";
+    case GLST_ERR_CUDA: return "CUDA error";
+    case GLST_ERR_NO_DEVICE: return "no CUDA device";
+    case GLST_ERR_TDESIGN: return "spherical t-design unavailable";
+    case GLST_ERR_NO_CONVERGENCE: return "no convergence";
+    case GLST_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case GLST_ERR_SIZE: return "size limit exceeded";
+    case GLST_ERR_STATE: return "invalid state";
+  }
+  return "unknown";
+}
+
+const char *glst_version(void) { return "glst-b200 0.1 (sm_100a)"; }
+
+uint32_t glst_max_atoms_per_cell(void) { return dev::kSortCap; }
+
+glst_status glst_set_tdesign_path(const char *path) {
+  std::lock_guard<std::mutex> lk(g_store_mu);
+  g_store_path = path ? path : "";
+  return GLST_OK;
+}
+
+glst_status glst_create(glst_handle **out, uint32_t natom, double tol, double bx, double by,
+                        double bz, double rcut, glst_ct ct) {
+  if (!out) return fail(GLST_ERR_INVALID_ARG, "null handle pointer");
+  *out = nullptr;
+  if (ct != GLST_CT_DOUBLE && ct != GLST_CT_FLOAT) return fail(GLST_ERR_INVALID_ARG, "bad calculation type");
+  auto h = std::make_unique<glst_handle>();
+  const double box[3] = {bx, by, bz};
+  glst_status s = setup(h.get(), natom, tol, box, rcut, ct == GLST_CT_FLOAT);
+  if (s != GLST_OK) {
+    release(h.get());
+    return s;
+  }
+  *out = h.release();
+  return GLST_OK;
+}
+
+glst_status glst_create_ncell(glst_handle **out, uint32_t natom, double tol, double bx, double by,
+                              double bz, uint32_t ncx, uint32_t ncy, uint32_t ncz, glst_ct ct) {
+  if (!ncx || !ncy || !ncz) return fail(GLST_ERR_INVALID_ARG, "cell counts must be > 0");
+  const double box[3] = {bx, by, bz};
+  const uint32_t nc[3] = {ncx, ncy, ncz};
+  return glst_create(out, natom, tol, bx, by, bz, glst::rcut_from_ncell(box, nc), ct);
+}
+
+glst_status glst_init(glst_handle *h, uint32_t natom, double tol, double bx, double by, double bz,
+                      double rcut) {
+  if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  const int ct = h->plan.ct_float;
+  CUDA_TRY(cudaDeviceSynchronize());
+  release(h);
+  const double box[3] = {bx, by, bz};
+  return setup(h, natom, tol, box, rcut, ct);
+}
+
+glst_status glst_destroy(glst_handle *h) {
+  if (!h) return GLST_OK;
+  cudaDeviceSynchronize();
+  release(h);
+  delete h;
+  return GLST_OK;
+}
+
+glst_status glst_compute(glst_handle *h, const double *rx, const double *ry, const double *rz,
+                         const double *qc, void *stream) {
+  if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  return compute_all(h, rx, ry, rz, qc, S_(stream));
+}
+
+glst_status glst_assign_atoms(glst_handle *h, const double *rx, const double *ry, const double *rz,
+                              const double *qc, void *stream) {
+  if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  return phase_assign(h, rx, ry, rz, qc, S_(stream));
+}
+glst_status glst_calc_sf(glst_handle *h, void *stream) {
+  if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  return phase_sf(h, S_(stream));
+}
+glst_status glst_sum_rmt_sf(glst_handle *h, void *stream) {
+  if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  return phase_shell(h, S_(stream));
+}
+glst_status glst_calc_lr_ef(glst_handle *h, void *stream) {
+  if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  return phase_lr(h, S_(stream));
+}
+glst_status glst_calc_sr_ef(glst_handle *h, void *stream) {
+  if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  return phase_sr(h, S_(stream));
+}
+glst_status glst_comm_ef(glst_handle *h, void *stream) {
+  if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  return phase_combine(h, S_(stream));
+}
+
+glst_status glst_get_ef(glst_handle *h, double *fx, double *fy, double *fz, double *en,
+                        int on_device, void *stream) {
+  if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  if (!h->computed) return fail(GLST_ERR_STATE, "get_ef called before a compute");
+  const size_t bytes = (size_t)h->plan.natom * sizeof(double);
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  cudaStream_t st = S_(stream);
+  double *dst[4] = {fx, fy, fz, en};
+  double *src[4] = {h->ofx, h->ofy, h->ofz, h->oen};
+  for (int i = 0; i < 4; i++)
+    if (dst[i] && bytes) CUDA_TRY(cudaMemcpyAsync(dst[i], src[i], bytes, kind, st));
+  if (!on_device) CUDA_TRY(cudaStreamSynchronize(st));
+  return GLST_OK;
+}
+
+glst_status glst_cell_outputs(glst_handle *h, double **fx, double **fy, double **fz, double **en) {
+  if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  if (fx) *fx = h->cfx;
+  if (fy) *fy = h->cfy;
+  if (fz) *fz = h->cfz;
+  if (en) *en = h->cen;
+  return GLST_OK;
+}
+
+glst_status glst_energy(glst_handle *h, double *e, void *stream) {
+  if (!h || !e) return fail(GLST_ERR_INVALID_ARG, "null argument");
+  if (!h->computed) return fail(GLST_ERR_STATE, "energy requested before a compute");
+  CUDA_TRY(cudaMemcpyAsync(e, h->energy, sizeof(double), cudaMemcpyDeviceToHost, S_(stream)));
+  CUDA_TRY(cudaStreamSynchronize(S_(stream)));
+  return GLST_OK;
+}
+
+glst_status glst_compute_host(glst_handle *h, const double *rx, const double *ry, const double *rz,
+                              const double *qc, double *fx, double *fy, double *fz, double *en,
+                              void *stream) {
+  if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  const size_t N = h->plan.natom, bytes = N * sizeof(double);
+  cudaStream_t st = S_(stream);
+  if (N && (!rx || !ry || !rz || !qc)) return fail(GLST_ERR_INVALID_ARG, "null input pointer");
+  const double *src[4] = {rx, ry, rz, qc};
+  for (int i = 0; i < 4; i++)
+    if (bytes) CUDA_TRY(cudaMemcpyAsync(h->in_host + i * N, src[i], bytes, cudaMemcpyHostToDevice, st));
+  GLST_TRY(compute_all(h, h->in_host, h->in_host + N, h->in_host + 2 * N, h->in_host + 3 * N, st));
+  return glst_get_ef(h, fx, fy, fz, en, 0, stream);
+}
+
+glst_status glst_get_assignment(glst_handle *h, uint32_t *sorted_idx, uint32_t *cell_count,
+                                uint32_t *cell_point) {
+  if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  CUDA_TRY(cudaDeviceSynchronize());
+  if (sorted_idx && h->plan.natom)
+    CUDA_TRY(cudaMemcpy(sorted_idx, h->sorted_idx, h->plan.natom * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  if (cell_count)
+    CUDA_TRY(cudaMemcpy(cell_count, h->cell_count, h->plan.ncell * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  if (cell_point)
+    CUDA_TRY(cudaMemcpy(cell_point, h->cell_point, h->plan.ncell * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  return GLST_OK;
+}
+
+static void fill_info(const Plan &p, glst_info *info) {
+  std::memset(info, 0, sizeof *info);
+  info->natom = p.natom;
+  for (int a = 0; a < 3; a++) info->ncell[a] = p.n[a];
+  info->ncell_total = p.ncell;
+  info->cell_dim = p.cell_dim;
+  info->ngroup = (uint32_t)p.groups.size();
+  info->num_nodes = p.K();
+  info->has_far_field = p.has_far ? 1u : 0u;
+  for (size_t g = 0; g < p.groups.size() && g < 16; g++) {
+    const auto &G = p.groups[g];
+    info->group_nodes[g] = G.n_radial * G.n_dir;
+    info->group_gl_degree[g] = G.gl_degree;
+    info->group_t_degree[g] = G.t_degree;
+    info->group_alpha[g] = G.alpha;
+    info->group_zcut[g] = G.zcut;
+    info->group_rmax[g] = G.rmax;
+    info->group_r_in[g] = G.r_in;
+    info->group_r_out[g] = G.r_out;
+  }
+}
+
+glst_status glst_get_info(const glst_handle *h, glst_info *info) {
+  if (!h || !info) return fail(GLST_ERR_INVALID_ARG, "null argument");
+  fill_info(h->plan, info);
+  info->device_bytes = h->bytes;
+  return GLST_OK;
+}
+
+glst_status glst_plan(uint32_t natom, double tol, double bx, double by, double bz, double rcut,
+                      glst_ct ct, glst_info *info, double *kx, double *ky, double *kz, double *w,
+                      uint32_t *group) {
+  if (!info) return fail(GLST_ERR_INVALID_ARG, "null info");
+  if (ct != GLST_CT_DOUBLE && ct != GLST_CT_FLOAT) return fail(GLST_ERR_INVALID_ARG, "bad calculation type");
+  const double box[3] = {bx, by, bz};
+  Plan p;
+  try {
+    auto store = get_store();
+    p = glst::make_plan(natom, tol, box, rcut, ct == GLST_CT_FLOAT, *store);
+  } catch (const PlanError &e) {
+    return fail(static_cast<glst_status>(e.status), "%s", e.msg.c_str());
+  } catch (const std::exception &e) {
+    return fail(GLST_ERR_TDESIGN, "planning failed: %s", e.what());
+  }
+  fill_info(p, info);
+  const size_t K = p.K();
+  if (kx) std::memcpy(kx, p.kx.data(), K * sizeof(double));
+  if (ky) std::memcpy(ky, p.ky.data(), K * sizeof(double));
+  if (kz) std::memcpy(kz, p.kz.data(), K * sizeof(double));
+  if (w) std::memcpy(w, p.w.data(), K * sizeof(double));
+  if (group) std::memcpy(group, p.group.data(), K * sizeof(uint32_t));
+  return GLST_OK;
+}
+
+glst_status glst_get_nodes(const glst_handle *h, double *kx, double *ky, double *kz, double *w,
+                           uint32_t *group) {
+  if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  const Plan &p = h->plan;
+  const size_t K = p.K();
+  if (kx) std::memcpy(kx, p.kx.data(), K * sizeof(double));
+  if (ky) std::memcpy(ky, p.ky.data(), K * sizeof(double));
+  if (kz) std::memcpy(kz, p.kz.data(), K * sizeof(double));
+  if (w) std::memcpy(w, p.w.data(), K * sizeof(double));
+  if (group) std::memcpy(group, p.group.data(), K * sizeof(uint32_t));
+  return GLST_OK;
+}
+
+glst_status glst_measure_pipe_peaks(double *sfu_per_s, double *fma_per_s) {
+  int device = 0, nsm = 0;
+  CUDA_TRY(cudaGetDevice(&device));
+  CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  const int threads = 512, blocks = nsm * 4, iters = 4096;
+  float *buf = nullptr;
+  CUDA_TRY(cudaMalloc(&buf, sizeof(float) * threads * blocks));
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  float best_sfu = 1e30f, best_fma = 1e30f, ms = 0.f;
+  for (int rep = 0; rep < 4; rep++) {
+    cudaEventRecord(a);
+    dev::k_probe_sfu<<<blocks, threads>>>(buf, iters);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&ms, a, b);
+    if (rep) best_sfu = std::min(best_sfu, ms);
+    cudaEventRecord(a);
+    dev::k_probe_fma<<<blocks, threads>>>(buf, iters * 4);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&ms, a, b);
+    if (rep) best_fma = std::min(best_fma, ms);
+  }
+  cudaError_t e = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(buf);
+  if (e != cudaSuccess) return fail(GLST_ERR_CUDA, "pipe probe failed: %s", cudaGetErrorString(e));
+  const double n = (double)threads * blocks * 8.0;
+  if (sfu_per_s) *sfu_per_s = n * iters * 2.0 / (best_sfu * 1e-3);
+  if (fma_per_s) *fma_per_s = n * iters * 4.0 / (best_fma * 1e-3);
+  return GLST_OK;
+}
+
+glst_status glst_check(glst_handle *h, void *stream) {
+  if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  uint32_t flags[4] = {0, 0, 0, 0};
+  CUDA_TRY(cudaMemcpyAsync(flags, h->flags, sizeof flags, cudaMemcpyDeviceToHost, S_(stream)));
+  CUDA_TRY(cudaStreamSynchronize(S_(stream)));
+  if (flags[0] & dev::kFlagCellOverflow)
+    return fail(GLST_ERR_SIZE,
+                "a cell holds more than %u atoms: energies and forces are valid but the "
+                "order of atoms inside that cell is not the reference's", dev::kSortCap);
+  return GLST_OK;
+}
+
+}  // extern "C"

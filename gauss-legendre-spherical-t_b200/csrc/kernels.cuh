@@ -1,0 +1,561 @@
+// GLST device kernels for sm_100a (B200).
+//
+// Data layout in HBM (one system):
+//   pk[N]      float4 (dx, dy, dz, q): cell-ordered atoms, position relative
+//              to the centre of the atom's cell, computed in FP64 and rounded
+//   pd[N]      double4 (x, y, z, q): cell-ordered atoms, FP64 absolute
+//   S[C][K]    double2: structure factor of every cell at every node
+//   R[C][K]    float2: shell sum times weight times e^{+ik.c} (cell centre c)
+//   part[P][N] double4: long-range partial sums, one row per node split
+//   sr[N]      double4: near-field sums
+// Cell c = (ix*ny + iy)*nz + iz, as in the reference (src/glst_force.cu:379-382).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace glst {
+namespace dev {
+
+constexpr unsigned kSortCap = 8192;   // atoms per cell the cell sort can hold
+constexpr unsigned kFlagCellOverflow = 1u;
+
+struct Grid {
+  uint32_t nx, ny, nz, ncell;
+  double l;       // cell edge (CT value widened to double)
+  int ct_float;   // bin in float arithmetic (glst_force<float>)
+};
+
+__device__ __forceinline__ double cell_centre(uint32_t i, double l) {
+  return (static_cast<double>(i) + 0.5) * l;
+}
+
+// ----------------------------------------------------------------------------
+// Cell assignment.  Binning follows calc_cell_atom_count_kernel
+// (src/glst_force.cu:356-386): the coordinate (converted to CT) times 1/l in
+// CT, truncated toward zero, clamped to [0, n-1].
+__device__ __forceinline__ uint32_t bin_axis(double r, const Grid &g, uint32_t n) {
+  int c;
+  if (g.ct_float) {
+    const float inv = __fdiv_rn(1.0f, static_cast<float>(g.l));
+    c = static_cast<int>(__fmul_rn(static_cast<float>(r), inv));
+  } else {
+    const double inv = __ddiv_rn(1.0, g.l);
+    c = static_cast<int>(__dmul_rn(r, inv));
+  }
+  c = (c >= static_cast<int>(n)) ? static_cast<int>(n) - 1 : c;
+  c = (c < 0) ? 0 : c;
+  return static_cast<uint32_t>(c);
+}
+
+// K_bin: cell of every atom and an (unordered) slot inside the cell.
+__global__ void k_bin(const double *__restrict__ rx, const double *__restrict__ ry,
+                      const double *__restrict__ rz, uint32_t n, Grid g,
+                      uint32_t *__restrict__ atom_cell, uint32_t *__restrict__ atom_slot,
+                      uint32_t *__restrict__ cell_count) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t cx = bin_axis(rx[i], g, g.nx);
+  const uint32_t cy = bin_axis(ry[i], g, g.ny);
+  const uint32_t cz = bin_axis(rz[i], g, g.nz);
+  const uint32_t cell = (cx * g.ny + cy) * g.nz + cz;
+  atom_cell[i] = cell;
+  atom_slot[i] = atomicAdd(&cell_count[cell], 1u);
+}
+
+// K_scan: exclusive offsets of the cell counts (one CTA of 1024 threads,
+// chunked block scan), and the error flag for cells the sort cannot hold.
+__global__ void k_scan(const uint32_t *__restrict__ cell_count, uint32_t ncell,
+                       uint32_t *__restrict__ cell_point, uint32_t *__restrict__ flags) {
+  __shared__ uint32_t warp_sums[32];
+  __shared__ uint32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  bool overflow = false;
+  for (uint32_t base = 0; base < ncell; base += blockDim.x) {
+    const uint32_t c = base + threadIdx.x;
+    const uint32_t v = (c < ncell) ? cell_count[c] : 0u;
+    overflow |= (v > kSortCap);
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= (unsigned)o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      const unsigned nw = blockDim.x >> 5;
+      uint32_t s = (lane < nw) ? warp_sums[lane] : 0u;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= (unsigned)o) s += y;
+      }
+      if (lane < nw) warp_sums[lane] = s;
+    }
+    __syncthreads();
+    const uint32_t before = carry + (warp ? warp_sums[warp - 1] : 0u) + (x - v);
+    if (c < ncell) cell_point[c] = before;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = before + v;
+    __syncthreads();
+  }
+  if (__syncthreads_or(overflow) && threadIdx.x == 0) atomicOr(flags, kFlagCellOverflow);
+}
+
+__global__ void k_scatter(const uint32_t *__restrict__ atom_cell,
+                          const uint32_t *__restrict__ atom_slot,
+                          const uint32_t *__restrict__ cell_point, uint32_t n,
+                          uint32_t *__restrict__ perm) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  perm[cell_point[atom_cell[i]] + atom_slot[i]] = i;
+}
+
+// K_sort_pack: one CTA per cell.  The atomics of k_bin leave the atoms of a
+// cell in arbitrary order; sorting each cell's indices ascending reproduces
+// the order of a stable sort by cell id (the reference's CUB radix sort,
+// src/glst_force.cu:510-517).  Then writes the packets.
+__global__ void k_sort_pack(const uint32_t *__restrict__ perm,
+                            const uint32_t *__restrict__ cell_count,
+                            const uint32_t *__restrict__ cell_point, Grid g,
+                            const double *__restrict__ rx, const double *__restrict__ ry,
+                            const double *__restrict__ rz, const double *__restrict__ qc,
+                            uint32_t *__restrict__ sorted_idx, float4 *__restrict__ pk,
+                            double4 *__restrict__ pd) {
+  extern __shared__ uint32_t s_idx[];
+  const uint32_t cell = blockIdx.x;
+  const uint32_t cnt = cell_count[cell];
+  const uint32_t start = cell_point[cell];
+  if (cnt == 0) return;
+  const uint32_t ix = cell / (g.ny * g.nz), iy = (cell / g.nz) % g.ny, iz = cell % g.nz;
+  const double cx = cell_centre(ix, g.l), cy = cell_centre(iy, g.l), cz = cell_centre(iz, g.l);
+  if (cnt > kSortCap) {
+    // Too many atoms to sort in shared memory: pack in slot order (physics
+    // unchanged, within-cell order not the reference's; k_scan flagged it).
+    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+      const uint32_t a = perm[start + i];
+      const double x = rx[a], y = ry[a], z = rz[a], q = qc[a];
+      sorted_idx[start + i] = a;
+      pd[start + i] = make_double4(x, y, z, q);
+      pk[start + i] = make_float4(static_cast<float>(x - cx), static_cast<float>(y - cy),
+                                  static_cast<float>(z - cz), static_cast<float>(q));
+    }
+    return;
+  }
+  uint32_t np2 = 1;
+  while (np2 < cnt) np2 <<= 1;
+  for (uint32_t i = threadIdx.x; i < np2; i += blockDim.x)
+    s_idx[i] = (i < cnt) ? perm[start + i] : 0xffffffffu;
+  __syncthreads();
+  // bitonic sort, ascending
+  for (uint32_t k = 2; k <= np2; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = threadIdx.x; i < np2; i += blockDim.x) {
+        const uint32_t p = i ^ j;
+        if (p > i) {
+          const uint32_t a = s_idx[i], b = s_idx[p];
+          const bool up = ((i & k) == 0);
+          if ((a > b) == up) {
+            s_idx[i] = b;
+            s_idx[p] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+    const uint32_t a = s_idx[i];
+    const double x = rx[a], y = ry[a], z = rz[a], q = qc[a];
+    sorted_idx[start + i] = a;
+    pd[start + i] = make_double4(x, y, z, q);
+    pk[start + i] = make_float4(static_cast<float>(x - cx), static_cast<float>(y - cy),
+                                static_cast<float>(z - cz), static_cast<float>(q));
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Structure factors.  S_c(k) = sum_{j in c} q_j e^{-i k.r_j}
+//                            = e^{-i k.c} sum_j q_j e^{-i k.d_j},  d_j = r_j - c.
+// The inner sum runs in FP32 on cell-relative coordinates (|k.d| <~ 25 rad,
+// SFU sincos); the twiddle e^{-ik.c} and the result are FP64.
+// CTA: 128 threads x 2 nodes; loops over kCellsPerCta consecutive cells.
+constexpr int kSfThreads = 128;
+constexpr int kSfNodesPerThread = 2;
+constexpr int kSfCellsPerCta = 8;
+constexpr int kSfAtomTile = 128;
+
+__global__ void __launch_bounds__(kSfThreads)
+k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_count,
+                    const uint32_t *__restrict__ cell_point, Grid g,
+                    const float4 *__restrict__ node32, const double4 *__restrict__ node64,
+                    uint32_t K, double2 *__restrict__ S) {
+  __shared__ float4 s_at[kSfAtomTile];
+  float kx[kSfNodesPerThread], ky[kSfNodesPerThread], kz[kSfNodesPerThread];
+  double Kx[kSfNodesPerThread], Ky[kSfNodesPerThread], Kz[kSfNodesPerThread];
+  bool act[kSfNodesPerThread];
+#pragma unroll
+  for (int u = 0; u < kSfNodesPerThread; u++) {
+    const uint32_t k = blockIdx.x * (kSfThreads * kSfNodesPerThread) + u * kSfThreads + threadIdx.x;
+    act[u] = k < K;
+    const float4 a = act[u] ? node32[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const double4 b = act[u] ? node64[k] : make_double4(0., 0., 0., 0.);
+    kx[u] = a.x; ky[u] = a.y; kz[u] = a.z;
+    Kx[u] = b.x; Ky[u] = b.y; Kz[u] = b.z;
+  }
+  const uint32_t c0 = blockIdx.y * kSfCellsPerCta;
+  const uint32_t c1 = min(g.ncell, c0 + kSfCellsPerCta);
+  for (uint32_t cell = c0; cell < c1; cell++) {
+    const uint32_t cnt = cell_count[cell];
+    const uint32_t start = cell_point[cell];
+    double sr[kSfNodesPerThread], si[kSfNodesPerThread];
+#pragma unroll
+    for (int u = 0; u < kSfNodesPerThread; u++) { sr[u] = 0.0; si[u] = 0.0; }
+    for (uint32_t a0 = 0; a0 < cnt; a0 += kSfAtomTile) {
+      const uint32_t na = min((uint32_t)kSfAtomTile, cnt - a0);
+      __syncthreads();
+      if (threadIdx.x < na) s_at[threadIdx.x] = pk[start + a0 + threadIdx.x];
+      __syncthreads();
+      float fr[kSfNodesPerThread], fi[kSfNodesPerThread];
+#pragma unroll
+      for (int u = 0; u < kSfNodesPerThread; u++) { fr[u] = 0.f; fi[u] = 0.f; }
+      for (uint32_t j = 0; j < na; j++) {
+        const float4 p = s_at[j];
+#pragma unroll
+        for (int u = 0; u < kSfNodesPerThread; u++) {
+          const float th = fmaf(kx[u], p.x, fmaf(ky[u], p.y, kz[u] * p.z));
+          float s, c;
+          __sincosf(th, &s, &c);
+          fr[u] = fmaf(p.w, c, fr[u]);
+          fi[u] = fmaf(-p.w, s, fi[u]);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kSfNodesPerThread; u++) { sr[u] += fr[u]; si[u] += fi[u]; }
+    }
+    const uint32_t ix = cell / (g.ny * g.nz), iy = (cell / g.nz) % g.ny, iz = cell % g.nz;
+    const double cx = cell_centre(ix, g.l), cy = cell_centre(iy, g.l), cz = cell_centre(iz, g.l);
+#pragma unroll
+    for (int u = 0; u < kSfNodesPerThread; u++) {
+      if (!act[u]) continue;
+      const uint32_t k = blockIdx.x * (kSfThreads * kSfNodesPerThread) + u * kSfThreads + threadIdx.x;
+      double ts, tc;
+      sincos(Kx[u] * cx + Ky[u] * cy + Kz[u] * cz, &ts, &tc);
+      // (sr + i si) * (tc - i ts)
+      S[(size_t)cell * K + k] = make_double2(sr[u] * tc + si[u] * ts, si[u] * tc - sr[u] * ts);
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Shell sums (src/glst_force.cu:702-913 restated for shared memory): per
+// node, an inclusive 3-D prefix sum of S over the cell grid (z, y, x), then
+// R_c = w * [box(c, r_out) - box(c, r_in)], 8 corners per box, clipped to the
+// grid.  All FP64.  Output R'_c(k) = R_c(k) e^{+ik.c} as float2.
+// CTA: nb nodes at once (nb = shared-memory budget / (16 C)), 256 threads.
+constexpr int kSatThreads = 256;
+
+struct SatArgs {
+  const double2 *S;
+  const double4 *node64;        // (kx, ky, kz, w) FP64
+  const uint32_t *node_radii;   // r_in | r_out << 16
+  uint32_t K;
+  uint32_t nb;                  // nodes per CTA
+  uint32_t stride;              // shared row stride (complex) = ncell + 1
+  float2 *R;
+};
+
+__device__ __forceinline__ double2 sat_at(const double2 *row, uint32_t x, uint32_t y,
+                                          uint32_t z, const Grid &g) {
+  return row[(x * g.ny + y) * g.nz + z];
+}
+
+__device__ __forceinline__ double2 cube_sum(const double2 *row, uint32_t x, uint32_t y,
+                                            uint32_t z, uint32_t r, const Grid &g) {
+  const uint32_t x0 = (x < r) ? 0 : x - r, y0 = (y < r) ? 0 : y - r, z0 = (z < r) ? 0 : z - r;
+  const uint32_t x1 = min(x + r, g.nx - 1), y1 = min(y + r, g.ny - 1), z1 = min(z + r, g.nz - 1);
+  const bool xb = x0 == 0, yb = y0 == 0, zb = z0 == 0;
+  const uint32_t xm = xb ? 0 : x0 - 1, ym = yb ? 0 : y0 - 1, zm = zb ? 0 : z0 - 1;
+  double2 s = sat_at(row, x1, y1, z1, g);
+  double2 t;
+  if (!xb) { t = sat_at(row, xm, y1, z1, g); s.x -= t.x; s.y -= t.y; }
+  if (!yb) { t = sat_at(row, x1, ym, z1, g); s.x -= t.x; s.y -= t.y; }
+  if (!zb) { t = sat_at(row, x1, y1, zm, g); s.x -= t.x; s.y -= t.y; }
+  if (!xb && !yb) { t = sat_at(row, xm, ym, z1, g); s.x += t.x; s.y += t.y; }
+  if (!xb && !zb) { t = sat_at(row, xm, y1, zm, g); s.x += t.x; s.y += t.y; }
+  if (!yb && !zb) { t = sat_at(row, x1, ym, zm, g); s.x += t.x; s.y += t.y; }
+  if (!xb && !yb && !zb) { t = sat_at(row, xm, ym, zm, g); s.x -= t.x; s.y -= t.y; }
+  return s;
+}
+
+__global__ void __launch_bounds__(kSatThreads)
+k_shell_sums(Grid g, SatArgs a) {
+  extern __shared__ double2 s_sat[];
+  const uint32_t k0 = blockIdx.x * a.nb;
+  const uint32_t nb = min(a.nb, a.K - k0);
+  const uint32_t C = g.ncell;
+  // load S[c][k0 .. k0+nb) -> s_sat[j*stride + c]
+  for (uint32_t t = threadIdx.x; t < C * nb; t += blockDim.x) {
+    const uint32_t c = t / nb, j = t % nb;
+    s_sat[j * a.stride + c] = a.S[(size_t)c * a.K + k0 + j];
+  }
+  __syncthreads();
+  // prefix along z (lines indexed by node, x, y)
+  for (uint32_t t = threadIdx.x; t < nb * g.nx * g.ny; t += blockDim.x) {
+    const uint32_t j = t / (g.nx * g.ny), xy = t % (g.nx * g.ny);
+    double2 *row = s_sat + j * a.stride + xy * g.nz;
+    double2 acc = make_double2(0.0, 0.0);
+    for (uint32_t z = 0; z < g.nz; z++) { acc.x += row[z].x; acc.y += row[z].y; row[z] = acc; }
+  }
+  __syncthreads();
+  // prefix along y (lines indexed by node, x, z)
+  for (uint32_t t = threadIdx.x; t < nb * g.nx * g.nz; t += blockDim.x) {
+    const uint32_t j = t / (g.nx * g.nz), xz = t % (g.nx * g.nz);
+    const uint32_t x = xz / g.nz, z = xz % g.nz;
+    double2 *row = s_sat + j * a.stride;
+    double2 acc = make_double2(0.0, 0.0);
+    for (uint32_t y = 0; y < g.ny; y++) {
+      double2 &v = row[(x * g.ny + y) * g.nz + z];
+      acc.x += v.x; acc.y += v.y; v = acc;
+    }
+  }
+  __syncthreads();
+  // prefix along x (lines indexed by node, y, z)
+  for (uint32_t t = threadIdx.x; t < nb * g.ny * g.nz; t += blockDim.x) {
+    const uint32_t j = t / (g.ny * g.nz), yz = t % (g.ny * g.nz);
+    double2 *row = s_sat + j * a.stride + yz;
+    double2 acc = make_double2(0.0, 0.0);
+    const uint32_t step = g.ny * g.nz;
+    for (uint32_t x = 0; x < g.nx; x++) { acc.x += row[x * step].x; acc.y += row[x * step].y; row[x * step] = acc; }
+  }
+  __syncthreads();
+  // shell sums, weight and twiddle; consecutive threads -> consecutive nodes
+  for (uint32_t t = threadIdx.x; t < C * nb; t += blockDim.x) {
+    const uint32_t c = t / nb, j = t % nb, k = k0 + j;
+    const uint32_t x = c / (g.ny * g.nz), y = (c / g.nz) % g.ny, z = c % g.nz;
+    const uint32_t radii = a.node_radii[k];
+    const double2 *row = s_sat + j * a.stride;
+    const double2 o = cube_sum(row, x, y, z, radii >> 16, g);
+    const double2 i = cube_sum(row, x, y, z, radii & 0xffffu, g);
+    const double4 nk = a.node64[k];
+    const double sr = (o.x - i.x) * nk.w, si = (o.y - i.y) * nk.w;
+    double ts, tc;
+    sincos(nk.x * cell_centre(x, g.l) + nk.y * cell_centre(y, g.l) + nk.z * cell_centre(z, g.l), &ts, &tc);
+    a.R[(size_t)c * a.K + k] = make_float2(static_cast<float>(sr * tc - si * ts),
+                                           static_cast<float>(sr * ts + si * tc));
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Long-range gather (src/glst_force.cu:983-1135 restated):
+//   en_i = q_i Re sum_k e^{ik.d_i} R'_c(k),   f_i = q_i sum_k Im(...) k
+// CTA = (cell, node split); thread = atom of the cell; nodes staged through
+// shared memory in tiles; FP32 inside a tile, FP64 across tiles.
+constexpr int kLrThreads = 128;
+constexpr int kLrTile = 256;
+
+__global__ void __launch_bounds__(kLrThreads)
+k_long_range(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_count,
+             const uint32_t *__restrict__ cell_point, const float4 *__restrict__ node32,
+             const float2 *__restrict__ R, uint32_t K, uint32_t nodes_per_split, uint32_t natom,
+             double4 *__restrict__ part) {
+  __shared__ float4 s_k[kLrTile];
+  __shared__ float2 s_r[kLrTile];
+  const uint32_t cell = blockIdx.x;
+  const uint32_t cnt = cell_count[cell];
+  const uint32_t start = cell_point[cell];
+  const uint32_t kb = blockIdx.y * nodes_per_split;
+  const uint32_t ke = min(K, kb + nodes_per_split);
+  const uint32_t nwarps_needed = (cnt + 31) / 32;
+  for (uint32_t a0 = 0; a0 < cnt; a0 += kLrThreads) {
+    // warps with no atom in this chunk skip the arithmetic but keep staging
+    const uint32_t ai = a0 + threadIdx.x;
+    const bool active = ai < cnt;
+    const bool warp_live = (a0 / 32 + (threadIdx.x >> 5)) < nwarps_needed;
+    float4 p = active ? pk[start + ai] : make_float4(0.f, 0.f, 0.f, 0.f);
+    double ex = 0.0, ey = 0.0, ez = 0.0, ee = 0.0;
+    for (uint32_t t0 = kb; t0 < ke; t0 += kLrTile) {
+      const uint32_t nt = min((uint32_t)kLrTile, ke - t0);
+      __syncthreads();
+      for (uint32_t t = threadIdx.x; t < nt; t += kLrThreads) {
+        s_k[t] = node32[t0 + t];
+        s_r[t] = R[(size_t)cell * K + t0 + t];
+      }
+      __syncthreads();
+      if (!warp_live) continue;
+      float fx = 0.f, fy = 0.f, fz = 0.f, fe = 0.f;
+#pragma unroll 4
+      for (uint32_t t = 0; t < nt; t++) {
+        const float4 k = s_k[t];
+        const float2 r = s_r[t];
+        const float th = fmaf(k.x, p.x, fmaf(k.y, p.y, k.z * p.z));
+        float s, c;
+        __sincosf(th, &s, &c);
+        const float dre = fmaf(c, r.x, -s * r.y);
+        const float dim = fmaf(c, r.y, s * r.x);
+        fe += dre;
+        fx = fmaf(dim, k.x, fx);
+        fy = fmaf(dim, k.y, fy);
+        fz = fmaf(dim, k.z, fz);
+      }
+      ex += fx; ey += fy; ez += fz; ee += fe;
+    }
+    if (active) {
+      const double q = static_cast<double>(p.w);
+      part[(size_t)blockIdx.y * natom + start + ai] = make_double4(q * ex, q * ey, q * ez, q * ee);
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Near field (src/glst_force.cu:1170-1544 restated): bare q_i q_j / r over
+// the own cell (self skipped) and the up to 26 neighbour cells inside the
+// grid (open boundary).  FP64 throughout.  CTA per cell, thread per atom.
+constexpr int kSrThreads = 128;
+
+__global__ void __launch_bounds__(kSrThreads)
+k_short_range(const double4 *__restrict__ pd, const uint32_t *__restrict__ cell_count,
+              const uint32_t *__restrict__ cell_point, Grid g, double4 *__restrict__ sr) {
+  __shared__ double4 s_at[kSrThreads];
+  const uint32_t cell = blockIdx.x;
+  const uint32_t cnt = cell_count[cell];
+  const uint32_t start = cell_point[cell];
+  const int ix = cell / (g.ny * g.nz), iy = (cell / g.nz) % g.ny, iz = cell % g.nz;
+  for (uint32_t a0 = 0; a0 < cnt; a0 += kSrThreads) {
+    const uint32_t ai = a0 + threadIdx.x;
+    const bool active = ai < cnt;
+    const double4 me = active ? pd[start + ai] : make_double4(0., 0., 0., 0.);
+    double fx = 0.0, fy = 0.0, fz = 0.0, en = 0.0;
+    // own cell first, then neighbours in (a, b, c) order as the reference
+    for (int nbi = -1; nbi < 27; nbi++) {
+      int dxc = 0, dyc = 0, dzc = 0;
+      if (nbi >= 0) {
+        if (nbi == 13) continue;  // (0,0,0) handled as nbi == -1
+        dxc = nbi / 9 - 1; dyc = (nbi / 3) % 3 - 1; dzc = nbi % 3 - 1;
+      }
+      const int jx = ix + dxc, jy = iy + dyc, jz = iz + dzc;
+      if (jx < 0 || jy < 0 || jz < 0 || jx >= (int)g.nx || jy >= (int)g.ny || jz >= (int)g.nz) continue;
+      const uint32_t nb = (jx * g.ny + jy) * g.nz + jz;
+      const uint32_t bcnt = cell_count[nb];
+      const uint32_t bstart = cell_point[nb];
+      for (uint32_t b0 = 0; b0 < bcnt; b0 += kSrThreads) {
+        const uint32_t nbt = min((uint32_t)kSrThreads, bcnt - b0);
+        __syncthreads();
+        if (threadIdx.x < nbt) s_at[threadIdx.x] = pd[bstart + b0 + threadIdx.x];
+        __syncthreads();
+        if (!active) continue;
+        for (uint32_t j = 0; j < nbt; j++) {
+          if (nbi < 0 && b0 + j == ai) continue;  // self
+          const double4 o = s_at[j];
+          const double dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
+          const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+          const double ir = rsqrt(r2);
+          const double e = me.w * o.w * ir;
+          const double fs = e * ir * ir;
+          fx = fma(fs, dx, fx);
+          fy = fma(fs, dy, fy);
+          fz = fma(fs, dz, fz);
+          en += e;
+        }
+      }
+    }
+    if (active) sr[start + ai] = make_double4(fx, fy, fz, en);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Combine: near field + long-range partials (fixed order), write the
+// cell-ordered outputs and scatter to input order; per-CTA energy sums.
+constexpr int kCombineThreads = 256;
+
+__global__ void __launch_bounds__(kCombineThreads)
+k_combine(const double4 *__restrict__ sr, const double4 *__restrict__ part, uint32_t nsplit,
+          const uint32_t *__restrict__ sorted_idx, uint32_t natom, int use_far,
+          double *__restrict__ cfx, double *__restrict__ cfy, double *__restrict__ cfz,
+          double *__restrict__ cen, double *__restrict__ ofx, double *__restrict__ ofy,
+          double *__restrict__ ofz, double *__restrict__ oen, double *__restrict__ block_energy) {
+  __shared__ double s_red[kCombineThreads / 32];
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0.0;
+  if (p < natom) {
+    double4 acc = make_double4(0., 0., 0., 0.);
+    if (use_far) {
+      for (uint32_t s = 0; s < nsplit; s++) {
+        const double4 v = part[(size_t)s * natom + p];
+        acc.x += v.x; acc.y += v.y; acc.z += v.z; acc.w += v.w;
+      }
+    }
+    const double4 v = sr[p];
+    acc.x += v.x; acc.y += v.y; acc.z += v.z; acc.w += v.w;
+    cfx[p] = acc.x; cfy[p] = acc.y; cfz[p] = acc.z; cen[p] = acc.w;
+    const uint32_t i = sorted_idx[p];
+    if (i < natom) { ofx[i] = acc.x; ofy[i] = acc.y; ofz[i] = acc.z; oen[i] = acc.w; }
+    e = acc.w;
+  }
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = e;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kCombineThreads / 32; w++) t += s_red[w];
+    block_energy[blockIdx.x] = t;
+  }
+}
+
+// Total energy 0.5 * sum of the per-CTA sums, fixed order (one CTA).
+__global__ void k_energy_total(const double *__restrict__ block_energy, uint32_t nblocks,
+                               double *__restrict__ total) {
+  __shared__ double s_red[32];
+  double e = 0.0;
+  for (uint32_t b = threadIdx.x; b < nblocks; b += blockDim.x) e += block_energy[b];
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = e;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (unsigned w = 0; w < (blockDim.x >> 5); w++) t += s_red[w];
+    *total = 0.5 * t;
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Pipe-peak probes (roofline denominators).  Eight independent chains per
+// thread keep the pipe busy; the results are stored so nothing is removed.
+__global__ void k_probe_sfu(float *out, int iters) {
+  float a[8];
+#pragma unroll
+  for (int u = 0; u < 8; u++) a[u] = 0.001f * (threadIdx.x + u);
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      float s, c;
+      __sincosf(a[u], &s, &c);
+      a[u] = s + c;  // 2 MUFU + 1 FADD
+    }
+  }
+  float t = 0.f;
+#pragma unroll
+  for (int u = 0; u < 8; u++) t += a[u];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = t;
+}
+
+__global__ void k_probe_fma(float *out, int iters) {
+  float a[8];
+#pragma unroll
+  for (int u = 0; u < 8; u++) a[u] = 0.001f * (threadIdx.x + u);
+  const float m = 0.999f, b = 0.0001f;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int u = 0; u < 8; u++) a[u] = fmaf(a[u], m, b);
+  }
+  float t = 0.f;
+#pragma unroll
+  for (int u = 0; u < 8; u++) t += a[u];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = t;
+}
+
+}  // namespace dev
+}  // namespace glst

@@ -1,0 +1,77 @@
+"""Seeded synthetic TIP3P-like water boxes (the inputs of every benchmark).
+
+Rigid water: O -0.834 e, H +0.417 e, O-H 0.9572 A, H-O-H 104.52 degrees.
+Oxygens sit on an m x m x m lattice of spacing L/m (m = ceil(n^(1/3)); when
+n < m^3 a seeded random subset of sites is used), jittered by U(-0.3, 0.3) A
+per axis; each molecule gets a uniformly random orientation (random unit
+quaternion).  Coordinates are FP64 and finally shifted so that the minimum
+coordinate on each axis is 0, as the reference's driver does before calling
+the library (utils/utils.cpp:35-58).  Atom order: O, H, H per molecule.
+"""
+import math
+
+import numpy as np
+
+Q_O, Q_H = -0.834, 0.417
+R_OH = 0.9572
+THETA_HOH = math.radians(104.52)
+
+# Standard configurations of the GLST benchmarks: (molecules, box edge A,
+# cutoff A, splitting alpha 1/A).  tol = erfc(alpha rcut) / rcut.
+CONFIGS = {
+    "water216": dict(n_mol=216, box=18.63, rcut=9.0, alpha=0.34),
+    "water10k": dict(n_mol=10000, box=66.9, rcut=10.0, alpha=0.31),
+    "water333k": dict(n_mol=333333, box=215.3, rcut=10.0, alpha=0.31),
+}
+
+
+def tol_from_alpha(alpha, rcut):
+    return math.erfc(alpha * rcut) / rcut
+
+
+def _random_rotations(rng, n):
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    R = np.empty((n, 3, 3))
+    R[:, 0, 0] = 1 - 2 * (y * y + z * z)
+    R[:, 0, 1] = 2 * (x * y - z * w)
+    R[:, 0, 2] = 2 * (x * z + y * w)
+    R[:, 1, 0] = 2 * (x * y + z * w)
+    R[:, 1, 1] = 1 - 2 * (x * x + z * z)
+    R[:, 1, 2] = 2 * (y * z - x * w)
+    R[:, 2, 0] = 2 * (x * z - y * w)
+    R[:, 2, 1] = 2 * (y * z + x * w)
+    R[:, 2, 2] = 1 - 2 * (x * x + y * y)
+    return R
+
+
+def water_box(n_mol, box, seed=0, recenter=True):
+    """Returns (x, y, z, q) FP64 arrays of 3*n_mol atoms."""
+    rng = np.random.default_rng(seed)
+    m = int(round(n_mol ** (1.0 / 3.0)))
+    while m ** 3 < n_mol:
+        m += 1
+    s = box / m
+    sites = np.stack(np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij"), -1).reshape(-1, 3)
+    if sites.shape[0] > n_mol:
+        sites = sites[np.sort(rng.choice(sites.shape[0], n_mol, replace=False))]
+    O = (sites + 0.5) * s + rng.uniform(-0.3, 0.3, size=(n_mol, 3))
+    half = 0.5 * THETA_HOH
+    local = np.array([[R_OH * math.sin(half), 0.0, R_OH * math.cos(half)],
+                      [-R_OH * math.sin(half), 0.0, R_OH * math.cos(half)]])
+    Rm = _random_rotations(rng, n_mol)
+    H = O[:, None, :] + np.einsum("nij,kj->nki", Rm, local)
+    pos = np.concatenate([O[:, None, :], H], axis=1).reshape(-1, 3)
+    q = np.tile(np.array([Q_O, Q_H, Q_H]), n_mol)
+    if recenter:
+        pos = pos - pos.min(axis=0)
+    return (np.ascontiguousarray(pos[:, 0]), np.ascontiguousarray(pos[:, 1]),
+            np.ascontiguousarray(pos[:, 2]), q)
+
+
+def config_system(name, seed=0):
+    c = CONFIGS[name]
+    x, y, z, q = water_box(c["n_mol"], c["box"], seed=seed)
+    return dict(x=x, y=y, z=z, q=q, box=(c["box"],) * 3, rcut=c["rcut"],
+                tol=tol_from_alpha(c["alpha"], c["rcut"]))

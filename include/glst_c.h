@@ -1,0 +1,193 @@
+/*
+ * glst_c.h -- C-ABI of the B200-native GLST electrostatics engine.
+ *
+ * One opaque handle replaces one `glst_force<CT>` object of the reference
+ * library (include/glst_force.hcu:24-125).  Every entry point takes plain
+ * pointers and sizes; CUDA streams are passed as `void*` (a cudaStream_t, or
+ * NULL for the legacy default stream).  No C++ or torch types cross this
+ * boundary and no exception escapes it: every call returns a glst_status and
+ * glst_last_error() gives the message of the last failure on this thread.
+ *
+ * Physics (same as the reference): open-boundary Coulomb energy and forces of
+ * point charges, in units of e^2/A (no Coulomb constant).  en[i] counts every
+ * pair from both sides, so the total energy is 0.5 * sum(en) (glst_energy).
+ *
+ * Differences from the reference's behaviour, all deliberate:
+ *   - outputs are overwritten by every compute call (the reference adds into
+ *     fx_/fy_/fz_/en_ and its caller zeroes them, test/full_example.cu:201-209);
+ *   - the compute path is fully stream ordered and never blocks the host
+ *     (the reference copies cell counts to the host every step,
+ *     src/glst_force.cu:474-482), so it can be captured in a CUDA graph;
+ *   - CUDA errors are always checked and returned (the reference ignores them
+ *     in release builds, include/cuda_utils.hcu:38-42).
+ */
+#ifndef GLST_C_H
+#define GLST_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum glst_status {
+  GLST_OK = 0,
+  GLST_ERR_INVALID_ARG = 1,   /* bad pointer, size or parameter */
+  GLST_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+  GLST_ERR_NO_DEVICE = 3,     /* no CUDA device */
+  GLST_ERR_TDESIGN = 4,       /* spherical t-design store missing / degree absent */
+  GLST_ERR_NO_CONVERGENCE = 5,/* GL rule / t-design / erfc inverse not found */
+  GLST_ERR_OUT_OF_MEMORY = 6, /* device allocation failed */
+  GLST_ERR_SIZE = 7,          /* a size limit of this build was exceeded */
+  GLST_ERR_STATE = 8          /* call out of order (e.g. get_ef before compute) */
+} glst_status;
+
+/* Calculation type of the reference object this handle stands in for.  It
+ * selects how the cell grid and the cell of each atom are computed (in float
+ * or double, src/glst_force.cu:223-241, :356-386) and the type the cubature
+ * nodes are rounded to (src/cubature.cu:138-141), so that the cell assignment
+ * is bit-identical to glst_force<float> or glst_force<double>.  The arithmetic
+ * of the sum itself is this engine's mixed precision in both cases. */
+typedef enum glst_ct { GLST_CT_DOUBLE = 0, GLST_CT_FLOAT = 1 } glst_ct;
+
+typedef struct glst_handle glst_handle;
+
+/* Plan summary (what the reference prints from init, src/glst_force.cu:245-293). */
+typedef struct glst_info {
+  uint32_t natom;
+  uint32_t ncell[3];
+  uint32_t ncell_total;
+  double cell_dim;          /* cell edge as the CT value, widened to double */
+  uint32_t ngroup;          /* alpha groups */
+  uint32_t num_nodes;       /* K, total cubature nodes */
+  uint32_t has_far_field;   /* 0 when some dimension has <= 2 cells */
+  uint32_t group_nodes[16]; /* nodes per group (first 16 groups) */
+  uint32_t group_gl_degree[16];
+  uint32_t group_t_degree[16];
+  double group_alpha[16];
+  double group_zcut[16];
+  double group_rmax[16];
+  uint32_t group_r_in[16];
+  uint32_t group_r_out[16];
+  uint64_t device_bytes;    /* device memory held by the handle */
+} glst_info;
+
+/* Where spherical t-designs are read from.  Either the project's binary store
+ * (tdesigns.bin) or a directory in the reference's text layout (the
+ * reference reads "SS31-Mar-2016/" in the working directory,
+ * src/cubature.cu:423-459, :490).  Default: the environment variable
+ * GLST_TDESIGN_PATH, else "SS31-Mar-2016/" if it exists in the working
+ * directory, else the store shipped next to the library.  Process-wide. */
+glst_status glst_set_tdesign_path(const char *path);
+
+/* glst_force(natom, tol, Lx, Ly, Lz, rcut)   src/glst_force.cu:72-78
+ * Plans cells, alpha groups and the cubature on the host (FP64) and
+ * allocates all device buffers on the current device. */
+glst_status glst_create(glst_handle **out, uint32_t natom, double tol,
+                        double box_x, double box_y, double box_z, double rcut,
+                        glst_ct ct);
+
+/* glst_force(natom, tol, Lx, Ly, Lz, ncx, ncy, ncz)   src/glst_force.cu:80-95
+ * rcut = min(L/n) over the three axes. */
+glst_status glst_create_ncell(glst_handle **out, uint32_t natom, double tol,
+                              double box_x, double box_y, double box_z,
+                              uint32_t ncell_x, uint32_t ncell_y,
+                              uint32_t ncell_z, glst_ct ct);
+
+/* glst_force::init(natom, tol, Lx, Ly, Lz, rcut)   src/glst_force.cu:179-327 */
+glst_status glst_init(glst_handle *h, uint32_t natom, double tol, double box_x,
+                      double box_y, double box_z, double rcut);
+
+/* ~glst_force()   src/glst_force.cu:97-100, :1768-1796 */
+glst_status glst_destroy(glst_handle *h);
+
+/* glst_force::calc_ener_force(d_rx, d_ry, d_rz, d_qc)   src/glst_force.cu:1604-1614
+ * Device pointers to natom FP64 values each (positions in A, charges in e),
+ * caller owned, read during the call only.  Stream ordered; returns without
+ * waiting for the GPU. */
+glst_status glst_compute(glst_handle *h, const double *d_rx, const double *d_ry,
+                         const double *d_rz, const double *d_qc, void *stream);
+
+/* The six phases of calc_ener_force, for callers of the reference's phase
+ * methods (include/glst_force.hcu:52-58).  Run in this order they produce
+ * exactly what glst_compute produces. */
+glst_status glst_assign_atoms(glst_handle *h, const double *d_rx,
+                              const double *d_ry, const double *d_rz,
+                              const double *d_qc, void *stream); /* :431-534 */
+glst_status glst_calc_sf(glst_handle *h, void *stream);      /* :666-700 */
+glst_status glst_sum_rmt_sf(glst_handle *h, void *stream);   /* :915-981 */
+glst_status glst_calc_lr_ef(glst_handle *h, void *stream);   /* :1137-1168 */
+glst_status glst_calc_sr_ef(glst_handle *h, void *stream);   /* :1546-1582 */
+glst_status glst_comm_ef(glst_handle *h, void *stream);      /* :1584-1602 */
+
+/* glst_force::get_ef(fx, fy, fz, en)   src/glst_force.cu:142-176
+ * Copies forces and per-atom energies in INPUT order into the four arrays
+ * (natom doubles each).  `on_device` = 0: host pointers, the call waits for
+ * the stream; 1: device pointers, stream ordered.  Any pointer may be NULL. */
+glst_status glst_get_ef(glst_handle *h, double *fx, double *fy, double *fz,
+                        double *en, int on_device, void *stream);
+
+/* Device pointers to the CELL-ordered outputs, as the reference's
+ * fx()/fy()/fz()/en() accessors return them (include/glst_force.hcu:36-43). */
+glst_status glst_cell_outputs(glst_handle *h, double **fx, double **fy,
+                              double **fz, double **en);
+
+/* Total energy 0.5 * sum_i en_i, reduced on the device in a fixed order
+ * (waits for the stream).  The reference leaves this sum to its caller. */
+glst_status glst_energy(glst_handle *h, double *e_total, void *stream);
+
+/* End to end from HOST memory: copies positions and charges to the device,
+ * computes, and copies forces/energies (input order) back; waits for the
+ * stream.  Equivalent to H2D + glst_compute + glst_get_ef(on_device=0). */
+glst_status glst_compute_host(glst_handle *h, const double *rx,
+                              const double *ry, const double *rz,
+                              const double *qc, double *fx, double *fy,
+                              double *fz, double *en, void *stream);
+
+/* Cell assignment of the last compute, copied to host arrays (waits):
+ * sorted_idx[natom] = input index of the atom at each cell-ordered slot
+ * (the reference's sorted_idx_), cell_count/cell_point[ncell] (its
+ * cell_atom_count_/cell_atom_point_).  Any pointer may be NULL. */
+glst_status glst_get_assignment(glst_handle *h, uint32_t *sorted_idx,
+                                uint32_t *cell_count, uint32_t *cell_point);
+
+glst_status glst_get_info(const glst_handle *h, glst_info *info);
+
+/* Cubature node set in the reference's order (group, radial, direction;
+ * src/cubature.cu:120-145), FP64 before any rounding to CT.  Arrays of
+ * info.num_nodes; any pointer may be NULL. */
+glst_status glst_get_nodes(const glst_handle *h, double *kx, double *ky,
+                           double *kz, double *w, uint32_t *group);
+
+/* Host-only planning, no device needed: the same cell grid, alpha groups and
+ * cubature glst_create would build (src/glst_force.cu:179-327).  Fills *info
+ * (device_bytes = 0) and, when non-NULL, the node arrays (info->num_nodes
+ * entries each; call once with NULL arrays to learn the count). */
+glst_status glst_plan(uint32_t natom, double tol, double box_x, double box_y,
+                      double box_z, double rcut, glst_ct ct, glst_info *info,
+                      double *kx, double *ky, double *kz, double *w,
+                      uint32_t *group);
+
+/* Measured pipe peaks of the current device, the denominators of the
+ * roofline of the phase kernels (which are bound by the SFU sin/cos and FP32
+ * pipes, not by tensor cores or HBM): `sfu_per_s` = MUFU sin+cos results per
+ * second, `fma_per_s` = FP32 fused multiply-adds per second, each from a
+ * dependent-chain loop over every SM.  Waits for the device. */
+glst_status glst_measure_pipe_peaks(double *sfu_per_s, double *fma_per_s);
+
+/* Device-side error flags raised by the last compute (bit 0: a cell held more
+ * atoms than this build's per-cell limit).  Waits for the stream. */
+glst_status glst_check(glst_handle *h, void *stream);
+
+/* Per-cell atom limit of this build (the cell sort runs in shared memory). */
+uint32_t glst_max_atoms_per_cell(void);
+
+const char *glst_last_error(void);
+const char *glst_status_string(glst_status s);
+const char *glst_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GLST_C_H */

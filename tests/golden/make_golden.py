@@ -1,0 +1,122 @@
+"""Generate the golden fixtures of this directory from the UNMODIFIED reference.
+
+Runs ``oracle/_ref/glst_ref_harness`` (the reference library compiled from its
+own sources by ``oracle/Makefile``; needs a CUDA GPU) on seeded synthetic water
+boxes and stores, per case, the inputs' recipe and the reference's outputs:
+per-atom fx, fy, fz, en in input order (glst_force<CT>::get_ef) and the cell
+assignment (sorted_idx_, cell_atom_count_, cell_atom_point_).
+
+The reference reads spherical t-designs from ``SS31-Mar-2016/`` in its working
+directory (src/cubature.cu:490); this script renders the project's store there
+(gauss-legendre-spherical-t_b200/data/tdesigns.bin) so both sides use the same
+nodes.
+
+    python tests/golden/make_golden.py [case ...]
+
+Output: tests/golden/<case>_<ct>.npz, plus a timing summary on stdout.
+"""
+import json
+import math
+import os
+import struct
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import __graft_entry__  # noqa: E402
+
+# case: (molecules, box A, rcut A, tol, seed); tol = erfc(alpha rcut)/rcut for
+# the named configurations
+CASES = {
+    "water216": (216, 18.63, 9.0, math.erfc(0.34 * 9.0) / 9.0, 0),
+    "w1000_tol1e-4": (1000, 31.04, 8.0, 1e-4, 3),
+    "w2000_tol1e-5": (2000, 39.1, 10.0, 1e-5, 5),
+    "water10k": (10000, 66.9, 10.0, math.erfc(0.31 * 10.0) / 10.0, 0),
+}
+CTS = ("double", "float")
+
+
+def harness():
+    return os.path.join(ROOT, "oracle", "_ref", "glst_ref_harness")
+
+
+def write_input(path, x, y, z, q, tol, L, rcut):
+    with open(path, "wb") as f:
+        f.write(struct.pack("<I", len(x)))
+        f.write(struct.pack("<d", tol))
+        f.write(struct.pack("<ddd", L, L, L))
+        f.write(struct.pack("<d", rcut))
+        for a in (x, y, z, q):
+            f.write(np.ascontiguousarray(a, dtype="<f8").tobytes())
+
+
+def read_output(path):
+    with open(path, "rb") as f:
+        data = f.read()
+    natom, K, nx, ny, nz, iters = struct.unpack_from("<6I", data, 0)
+    off = 24
+    ms = np.frombuffer(data, dtype="<f8", count=8, offset=off)
+    off += 64
+    arrs = []
+    for _ in range(4):
+        arrs.append(np.frombuffer(data, dtype="<f8", count=natom, offset=off).copy())
+        off += 8 * natom
+    sidx = np.frombuffer(data, dtype="<u4", count=natom, offset=off).copy()
+    off += 4 * natom
+    C = nx * ny * nz
+    cnt = np.frombuffer(data, dtype="<u4", count=C, offset=off).copy()
+    off += 4 * C
+    pnt = np.frombuffer(data, dtype="<u4", count=C, offset=off).copy()
+    return dict(natom=natom, K=K, ncell=(nx, ny, nz), iters=iters, ms=ms, fx=arrs[0], fy=arrs[1],
+                fz=arrs[2], en=arrs[3], sorted_idx=sidx, cell_count=cnt, cell_point=pnt)
+
+
+def render_tdesigns(dst):
+    g = __graft_entry__.load_package()
+    sys.path.insert(0, os.path.join(os.path.dirname(g.TDESIGN_STORE)))
+    import make_tdesigns
+    make_tdesigns.write_reference_dir(g.TDESIGN_STORE, os.path.join(dst, "SS31-Mar-2016"))
+
+
+def main(cases, iters=5):
+    g = __graft_entry__.load_package()
+    from glst_b200 import systems
+    if not os.path.exists(harness()):
+        raise SystemExit("build the reference first: make -C oracle ref")
+    summary = {}
+    with tempfile.TemporaryDirectory() as work:
+        render_tdesigns(work)
+        for case in cases:
+            n_mol, L, rcut, tol, seed = CASES[case]
+            x, y, z, q = systems.water_box(n_mol, L, seed=seed)
+            inp = os.path.join(work, case + ".in")
+            write_input(inp, x, y, z, q, tol, L, rcut)
+            for ct in CTS:
+                out = os.path.join(work, "%s_%s.out" % (case, ct))
+                r = subprocess.run([harness(), inp, out, ct, str(iters)], cwd=work, capture_output=True,
+                                   text=True)
+                if r.returncode != 0:
+                    print(r.stdout[-2000:], r.stderr[-2000:])
+                    raise SystemExit("reference harness failed on %s/%s (%d)" % (case, ct, r.returncode))
+                o = read_output(out)
+                np.savez_compressed(os.path.join(HERE, "%s_%s.npz" % (case, ct)),
+                                    n_mol=n_mol, box=L, rcut=rcut, tol=tol, seed=seed, K=o["K"],
+                                    ncell=np.array(o["ncell"]), fx=o["fx"], fy=o["fy"], fz=o["fz"], en=o["en"],
+                                    sorted_idx=o["sorted_idx"], cell_count=o["cell_count"],
+                                    cell_point=o["cell_point"], ref_ms=o["ms"])
+                summary["%s_%s" % (case, ct)] = dict(
+                    natom=o["natom"], K=o["K"], ncell=o["ncell"],
+                    ms=dict(zip(["assign", "sf", "sum_rmt", "lr", "sr", "comm", "total_host", "total_events"],
+                                [round(float(v), 4) for v in o["ms"]])))
+                print(json.dumps({case + "_" + ct: summary["%s_%s" % (case, ct)]}), flush=True)
+    return summary
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:] or list(CASES))
