@@ -368,6 +368,20 @@ static glst_status compute_all(glst_handle *h, const double *rx, const double *r
   return phase_combine(h, st);
 }
 
+// Entry points run on the handle's device whatever device is current, and
+// leave the caller's current device as they found it.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(const glst_handle *h) {
+    if (!h) return;
+    if (cudaGetDevice(&prev) == cudaSuccess && prev != h->device) cudaSetDevice(h->device);
+    else prev = -1;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
 // ---------------------------------------------------------------- C-ABI
 extern "C" {
 
@@ -425,6 +439,7 @@ glst_status glst_create_ncell(glst_handle **out, uint32_t natom, double tol, dou
 glst_status glst_init(glst_handle *h, uint32_t natom, double tol, double bx, double by, double bz,
                       double rcut) {
   if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  DeviceGuard guard_(h);
   const int ct = h->plan.ct_float;
   CUDA_TRY(cudaDeviceSynchronize());
   release(h);
@@ -434,6 +449,7 @@ glst_status glst_init(glst_handle *h, uint32_t natom, double tol, double bx, dou
 
 glst_status glst_destroy(glst_handle *h) {
   if (!h) return GLST_OK;
+  DeviceGuard guard_(h);
   cudaDeviceSynchronize();
   release(h);
   delete h;
@@ -443,38 +459,46 @@ glst_status glst_destroy(glst_handle *h) {
 glst_status glst_compute(glst_handle *h, const double *rx, const double *ry, const double *rz,
                          const double *qc, void *stream) {
   if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  DeviceGuard guard_(h);
   return compute_all(h, rx, ry, rz, qc, S_(stream));
 }
 
 glst_status glst_assign_atoms(glst_handle *h, const double *rx, const double *ry, const double *rz,
                               const double *qc, void *stream) {
   if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  DeviceGuard guard_(h);
   return phase_assign(h, rx, ry, rz, qc, S_(stream));
 }
 glst_status glst_calc_sf(glst_handle *h, void *stream) {
   if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  DeviceGuard guard_(h);
   return phase_sf(h, S_(stream));
 }
 glst_status glst_sum_rmt_sf(glst_handle *h, void *stream) {
   if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  DeviceGuard guard_(h);
   return phase_shell(h, S_(stream));
 }
 glst_status glst_calc_lr_ef(glst_handle *h, void *stream) {
   if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  DeviceGuard guard_(h);
   return phase_lr(h, S_(stream));
 }
 glst_status glst_calc_sr_ef(glst_handle *h, void *stream) {
   if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  DeviceGuard guard_(h);
   return phase_sr(h, S_(stream));
 }
 glst_status glst_comm_ef(glst_handle *h, void *stream) {
   if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  DeviceGuard guard_(h);
   return phase_combine(h, S_(stream));
 }
 
 glst_status glst_get_ef(glst_handle *h, double *fx, double *fy, double *fz, double *en,
                         int on_device, void *stream) {
   if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  DeviceGuard guard_(h);
   if (!h->computed) return fail(GLST_ERR_STATE, "get_ef called before a compute");
   const size_t bytes = (size_t)h->plan.natom * sizeof(double);
   const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
@@ -489,6 +513,7 @@ glst_status glst_get_ef(glst_handle *h, double *fx, double *fy, double *fz, doub
 
 glst_status glst_cell_outputs(glst_handle *h, double **fx, double **fy, double **fz, double **en) {
   if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  DeviceGuard guard_(h);
   if (fx) *fx = h->cfx;
   if (fy) *fy = h->cfy;
   if (fz) *fz = h->cfz;
@@ -498,6 +523,7 @@ glst_status glst_cell_outputs(glst_handle *h, double **fx, double **fy, double *
 
 glst_status glst_energy(glst_handle *h, double *e, void *stream) {
   if (!h || !e) return fail(GLST_ERR_INVALID_ARG, "null argument");
+  DeviceGuard guard_(h);
   if (!h->computed) return fail(GLST_ERR_STATE, "energy requested before a compute");
   CUDA_TRY(cudaMemcpyAsync(e, h->energy, sizeof(double), cudaMemcpyDeviceToHost, S_(stream)));
   CUDA_TRY(cudaStreamSynchronize(S_(stream)));
@@ -508,6 +534,7 @@ glst_status glst_compute_host(glst_handle *h, const double *rx, const double *ry
                               const double *qc, double *fx, double *fy, double *fz, double *en,
                               void *stream) {
   if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  DeviceGuard guard_(h);
   const size_t N = h->plan.natom, bytes = N * sizeof(double);
   cudaStream_t st = S_(stream);
   if (N && (!rx || !ry || !rz || !qc)) return fail(GLST_ERR_INVALID_ARG, "null input pointer");
@@ -521,6 +548,7 @@ glst_status glst_compute_host(glst_handle *h, const double *rx, const double *ry
 glst_status glst_get_assignment(glst_handle *h, uint32_t *sorted_idx, uint32_t *cell_count,
                                 uint32_t *cell_point) {
   if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  DeviceGuard guard_(h);
   CUDA_TRY(cudaDeviceSynchronize());
   if (sorted_idx && h->plan.natom)
     CUDA_TRY(cudaMemcpy(sorted_idx, h->sorted_idx, h->plan.natom * sizeof(uint32_t), cudaMemcpyDeviceToHost));
@@ -555,6 +583,7 @@ static void fill_info(const Plan &p, glst_info *info) {
 
 glst_status glst_get_info(const glst_handle *h, glst_info *info) {
   if (!h || !info) return fail(GLST_ERR_INVALID_ARG, "null argument");
+  DeviceGuard guard_(h);
   fill_info(h->plan, info);
   info->device_bytes = h->bytes;
   return GLST_OK;
@@ -588,6 +617,7 @@ glst_status glst_plan(uint32_t natom, double tol, double bx, double by, double b
 glst_status glst_get_nodes(const glst_handle *h, double *kx, double *ky, double *kz, double *w,
                            uint32_t *group) {
   if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  DeviceGuard guard_(h);
   const Plan &p = h->plan;
   const size_t K = p.K();
   if (kx) std::memcpy(kx, p.kx.data(), K * sizeof(double));
@@ -636,6 +666,7 @@ glst_status glst_measure_pipe_peaks(double *sfu_per_s, double *fma_per_s) {
 
 glst_status glst_check(glst_handle *h, void *stream) {
   if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  DeviceGuard guard_(h);
   uint32_t flags[4] = {0, 0, 0, 0};
   CUDA_TRY(cudaMemcpyAsync(flags, h->flags, sizeof flags, cudaMemcpyDeviceToHost, S_(stream)));
   CUDA_TRY(cudaStreamSynchronize(S_(stream)));

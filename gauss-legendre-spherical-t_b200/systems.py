@@ -75,3 +75,59 @@ def config_system(name, seed=0):
     x, y, z, q = water_box(c["n_mol"], c["box"], seed=seed)
     return dict(x=x, y=y, z=z, q=q, box=(c["box"],) * 3, rcut=c["rcut"],
                 tol=tol_from_alpha(c["alpha"], c["rcut"]))
+
+
+# ----------------------------------------------------------------- CHARMM IO
+# The reference's driver reads CHARMM extended-format files
+# (utils/io.cpp:35-117): the .psf header line holds natom in columns 0-9 and
+# "!NATOM" at column 11; each atom line holds the charge in columns 50-63.
+# The .cor file has '*' title lines, natom in columns 0-9, then x, y, z in
+# columns 40-59, 60-79 and 80-99.
+
+def write_charmm(prefix, x, y, z, q):
+    """Write <prefix>.psf and <prefix>.cor readable by the reference driver."""
+    n = len(x)
+    with open(prefix + ".psf", "w") as f:
+        f.write("PSF EXT\n\n         1 !NTITLE\n* synthetic TIP3P-like water\n\n")
+        f.write("%10d !NATOM\n" % n)
+        for i in range(n):
+            name = "OH2" if i % 3 == 0 else ("H1" if i % 3 == 1 else "H2")
+            head = "%10d WAT      %-8d TIP3     %-8s" % (i + 1, i // 3 + 1, name)
+            f.write(head.ljust(50)[:50] + "%14.6f" % q[i] + "%14.4f%12d\n" % (16.0 if i % 3 == 0 else 1.008, 0))
+    with open(prefix + ".cor", "w") as f:
+        f.write("* synthetic TIP3P-like water\n*\n")
+        f.write("%10d  EXT\n" % n)
+        for i in range(n):
+            name = "OH2" if i % 3 == 0 else ("H1" if i % 3 == 1 else "H2")
+            head = "%10d%10d  %-8s  %-8s" % (i + 1, i // 3 + 1, "TIP3", name)
+            f.write(head.ljust(40)[:40] + "%20.10f%20.10f%20.10f" % (x[i], y[i], z[i]) + "  WAT      %-8d  0.0000000000\n" % (i // 3 + 1))
+
+
+def read_charmm(prefix):
+    """(x, y, z, q) from <prefix>.psf/.cor, the columns the reference reads."""
+    natom = None
+    q = []
+    with open(prefix + ".psf") as f:
+        lines = f.read().split("\n")
+    it = iter(lines)
+    for line in it:
+        if len(line) >= 17 and line[11:17] == "!NATOM":
+            natom = int(line[0:11])
+            break
+    for _ in range(natom):
+        q.append(float(next(it)[50:64]))
+    with open(prefix + ".cor") as f:
+        lines = [ln for ln in f.read().split("\n")]
+    k = 0
+    while lines[k][:1] == "*" or not lines[k].strip():
+        k += 1
+    if int(lines[k][0:10]) != natom:
+        raise ValueError("atom count differs between .psf and .cor")
+    xyz = np.array([[float(ln[40:60]), float(ln[60:80]), float(ln[80:100])] for ln in lines[k + 1:k + 1 + natom]])
+    return (np.ascontiguousarray(xyz[:, 0]), np.ascontiguousarray(xyz[:, 1]),
+            np.ascontiguousarray(xyz[:, 2]), np.array(q))
+
+
+def recenter(x, y, z):
+    """Shift so the minimum coordinate on each axis is 0 (utils/utils.cpp:35-58)."""
+    return x - x.min(), y - y.min(), z - z.min()

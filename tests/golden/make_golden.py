@@ -42,6 +42,13 @@ CASES = {
 CTS = ("double", "float")
 
 
+def input_sha256(x, y, z, q):
+    """Digest of the FP64 inputs, so a test can tell that it regenerated the
+    same positions and charges the fixture was made from."""
+    import hashlib
+    return hashlib.sha256(b"".join(np.ascontiguousarray(a, dtype="<f8").tobytes() for a in (x, y, z, q))).hexdigest()
+
+
 def harness():
     return os.path.join(ROOT, "oracle", "_ref", "glst_ref_harness")
 
@@ -95,6 +102,7 @@ def main(cases, iters=5):
         for case in cases:
             n_mol, L, rcut, tol, seed = CASES[case]
             x, y, z, q = systems.water_box(n_mol, L, seed=seed)
+            digest = input_sha256(x, y, z, q)
             inp = os.path.join(work, case + ".in")
             write_input(inp, x, y, z, q, tol, L, rcut)
             for ct in CTS:
@@ -109,7 +117,7 @@ def main(cases, iters=5):
                                     n_mol=n_mol, box=L, rcut=rcut, tol=tol, seed=seed, K=o["K"],
                                     ncell=np.array(o["ncell"]), fx=o["fx"], fy=o["fy"], fz=o["fz"], en=o["en"],
                                     sorted_idx=o["sorted_idx"], cell_count=o["cell_count"],
-                                    cell_point=o["cell_point"], ref_ms=o["ms"])
+                                    cell_point=o["cell_point"], ref_ms=o["ms"], input_sha256=np.array(digest))
                 summary["%s_%s" % (case, ct)] = dict(
                     natom=o["natom"], K=o["K"], ncell=o["ncell"],
                     ms=dict(zip(["assign", "sf", "sum_rmt", "lr", "sr", "comm", "total_host", "total_events"],
