@@ -104,7 +104,7 @@ struct glst_handle {
   int device = 0;
   dev::Grid grid{};
   uint32_t K = 0;
-  uint32_t nsplit = 1, nodes_per_split = 0;
+  uint32_t nsplit = 1;  // long-range chunks (rows of part)
   uint32_t sat_nb = 1, sat_stride = 0;
   size_t sat_smem = 0;
   uint32_t combine_blocks = 1;
@@ -117,10 +117,13 @@ struct glst_handle {
   uint32_t *flags = nullptr;
   float4 *pk = nullptr;
   double4 *pd = nullptr;
-  // nodes
+  // nodes, internal order: group -> direction -> radial
   float4 *node32 = nullptr;
   double4 *node64 = nullptr;
   uint32_t *node_radii = nullptr;
+  float4 *dirs = nullptr;       // unit directions, FP32
+  float *kappa = nullptr;       // radial scales per group, FP32
+  dev::LrChunk *chunks = nullptr;
   // far field
   double2 *S = nullptr;
   float2 *R = nullptr;
@@ -188,29 +191,55 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
   h->K = p.has_far ? p.K() : 0;
   const size_t N = natom, C = p.ncell, K = h->K;
 
-  // Node arrays.  Nodes and weights are rounded to CT first, as the
-  // reference stores them (src/cubature.cu:138-141).
+  // Node arrays, in the internal order group -> direction -> radial (the
+  // reference's is group -> radial -> direction, src/cubature.cu:120-145).
+  // Nodes and weights are rounded to CT first, as the reference stores them
+  // (src/cubature.cu:138-141).
+  std::vector<uint32_t> kappa_base, dir_base, node_base;
   {
     std::vector<float4> n32(K);
     std::vector<double4> n64(K);
     std::vector<uint32_t> radii(K);
-    for (size_t k = 0; k < K; k++) {
-      double kx = p.kx[k], ky = p.ky[k], kz = p.kz[k], w = p.w[k];
-      if (p.ct_float) {
-        kx = (double)(float)kx; ky = (double)(float)ky; kz = (double)(float)kz; w = (double)(float)w;
+    std::vector<float4> dirs;
+    std::vector<float> kap;
+    uint32_t ref_base = 0, ibase = 0;
+    for (size_t gi = 0; gi < (K ? p.groups.size() : 0); gi++) {
+      const auto &g = p.groups[gi];
+      kappa_base.push_back((uint32_t)kap.size());
+      dir_base.push_back((uint32_t)dirs.size());
+      node_base.push_back(ibase);
+      for (unsigned r = 0; r < g.n_radial; r++) kap.push_back((float)g.kappa[r]);
+      for (unsigned j = 0; j < g.n_dir; j++)
+        dirs.push_back(make_float4((float)g.dirs[3 * j], (float)g.dirs[3 * j + 1], (float)g.dirs[3 * j + 2], 0.f));
+      for (unsigned j = 0; j < g.n_dir; j++) {
+        for (unsigned r = 0; r < g.n_radial; r++) {
+          const size_t ref = ref_base + (size_t)r * g.n_dir + j;
+          const size_t k = ibase + (size_t)j * g.n_radial + r;
+          double kx = p.kx[ref], ky = p.ky[ref], kz = p.kz[ref], w = p.w[ref];
+          if (p.ct_float) {
+            kx = (double)(float)kx; ky = (double)(float)ky; kz = (double)(float)kz; w = (double)(float)w;
+          }
+          n64[k] = make_double4(kx, ky, kz, w);
+          n32[k] = make_float4((float)kx, (float)ky, (float)kz, 0.f);
+          radii[k] = (g.r_in & 0xffffu) | (g.r_out << 16);
+        }
       }
-      n64[k] = make_double4(kx, ky, kz, w);
-      n32[k] = make_float4((float)kx, (float)ky, (float)kz, 0.f);
-      const auto &g = p.groups[p.group[k]];
-      radii[k] = (g.r_in & 0xffffu) | (g.r_out << 16);
+      ref_base += g.n_radial * g.n_dir;
+      ibase += g.n_radial * g.n_dir;
+      if (g.n_radial > (unsigned)dev::kLrTileNodes)
+        return fail(GLST_ERR_SIZE, "%u radial nodes exceed the tile of the long-range kernel", g.n_radial);
     }
     GLST_TRY(dalloc_n(h, &h->node32, K));
     GLST_TRY(dalloc_n(h, &h->node64, K));
     GLST_TRY(dalloc_n(h, &h->node_radii, K));
+    GLST_TRY(dalloc_n(h, &h->dirs, dirs.size()));
+    GLST_TRY(dalloc_n(h, &h->kappa, kap.size()));
     if (K) {
       CUDA_TRY(cudaMemcpy(h->node32, n32.data(), K * sizeof(float4), cudaMemcpyHostToDevice));
       CUDA_TRY(cudaMemcpy(h->node64, n64.data(), K * sizeof(double4), cudaMemcpyHostToDevice));
       CUDA_TRY(cudaMemcpy(h->node_radii, radii.data(), K * sizeof(uint32_t), cudaMemcpyHostToDevice));
+      CUDA_TRY(cudaMemcpy(h->dirs, dirs.data(), dirs.size() * sizeof(float4), cudaMemcpyHostToDevice));
+      CUDA_TRY(cudaMemcpy(h->kappa, kap.data(), kap.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
   }
   GLST_TRY(dalloc_n(h, &h->atom_cell, N));
@@ -222,7 +251,7 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
   GLST_TRY(dalloc_n(h, &h->flags, 4));
   GLST_TRY(dalloc_n(h, &h->pk, N));
   GLST_TRY(dalloc_n(h, &h->pd, N));
-  GLST_TRY(dalloc_n(h, &h->sr, N));
+  GLST_TRY(dalloc_n(h, &h->sr, (size_t)dev::kSrPlanes * N));
   for (double **o : {&h->cfx, &h->cfy, &h->cfz, &h->cen, &h->ofx, &h->ofy, &h->ofz, &h->oen})
     GLST_TRY(dalloc_n(h, o, N));
   h->combine_blocks = (uint32_t)std::max<size_t>(1, (N + dev::kCombineThreads - 1) / dev::kCombineThreads);
@@ -231,32 +260,51 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
   GLST_TRY(dalloc_n(h, &h->in_host, 4 * N));
 
   if (K) {
-    // Shared-memory plan of the shell-sum kernel: as many nodes per CTA as
-    // fit (rows of ncell+1 complex doubles), at most 32.
-    int smem_optin = 0;
+    // Shared-memory plan of the shell-sum kernel: per node a row of ncell+1
+    // complex doubles plus its twiddle tables; a few nodes per CTA when the
+    // grid is small (occupancy), one when it is large.
+    int smem_optin = 0, nsm = 148;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+    // row stride = 1 (mod 8) complex doubles: rows of consecutive nodes start
+    // 16 bytes apart modulo 128, so the node-fastest accesses of the shell
+    // pass spread over all shared-memory banks
     h->sat_stride = (uint32_t)(C + 1);
-    const size_t row = (size_t)h->sat_stride * sizeof(double2);
+    while (h->sat_stride % 8 != 1) h->sat_stride++;
+    const size_t per_node = ((size_t)h->sat_stride + p.n[0] + p.n[1] + p.n[2]) * sizeof(double2);
     const size_t budget = std::min<size_t>((size_t)smem_optin, 200 * 1024);
-    if (row > budget)
+    if (per_node > budget)
       return fail(GLST_ERR_SIZE,
                   "cell grid of %zu cells exceeds the shell-sum shared-memory limit (%zu cells)",
                   C, budget / sizeof(double2) - 1);
-    h->sat_nb = (uint32_t)std::min<size_t>(32, budget / row);
-    h->sat_smem = row * h->sat_nb;
+    h->sat_nb = (uint32_t)std::max<size_t>(1, std::min<size_t>(16, (100 * 1024) / per_node));
+    h->sat_smem = per_node * h->sat_nb;
     // one process-wide maximum, so handles with different plans coexist
     CUDA_TRY(cudaFuncSetAttribute(dev::k_shell_sums, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)budget));
-    // Node splits of the long-range gather: enough CTAs to fill the GPU.
-    int nsm = 148;
-    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
-    const size_t want = (size_t)nsm * 16;
-    size_t nsplit = (want + C - 1) / C;
-    nsplit = std::max<size_t>(1, std::min<size_t>(nsplit, (K + 1023) / 1024));
-    nsplit = std::min<size_t>(nsplit, 65535);
-    h->nodes_per_split = (uint32_t)((K + nsplit - 1) / nsplit);
-    h->nodes_per_split = ((h->nodes_per_split + dev::kLrTile - 1) / dev::kLrTile) * dev::kLrTile;
-    h->nsplit = (uint32_t)((K + h->nodes_per_split - 1) / h->nodes_per_split);
+    // Long-range chunks: whole directions of one group each, sized so that
+    // ncell x chunks is several waves of resident CTAs.
+    const size_t slots = (size_t)nsm * 16;
+    const size_t want_chunks = std::max<size_t>(1, (8 * slots + C - 1) / C);
+    const size_t target_nodes = std::max<size_t>(1, K / want_chunks);
+    std::vector<dev::LrChunk> chunks;
+    for (size_t gi = 0; gi < p.groups.size(); gi++) {
+      const auto &g = p.groups[gi];
+      const uint32_t dpc = (uint32_t)std::max<size_t>(1, target_nodes / g.n_radial);
+      for (uint32_t j0 = 0; j0 < g.n_dir; j0 += dpc) {
+        dev::LrChunk c{};
+        c.n_dir = std::min(dpc, g.n_dir - j0);
+        c.n_rad = g.n_radial;
+        c.node_begin = node_base[gi] + j0 * g.n_radial;
+        c.dir_begin = dir_base[gi] + j0;
+        c.kappa_begin = kappa_base[gi];
+        chunks.push_back(c);
+      }
+    }
+    if (chunks.size() > 65535) return fail(GLST_ERR_SIZE, "too many long-range chunks");
+    h->nsplit = (uint32_t)chunks.size();
+    GLST_TRY(dalloc_n(h, &h->chunks, chunks.size()));
+    CUDA_TRY(cudaMemcpy(h->chunks, chunks.data(), chunks.size() * sizeof(dev::LrChunk), cudaMemcpyHostToDevice));
     GLST_TRY(dalloc_n(h, &h->S, C * K));
     GLST_TRY(dalloc_n(h, &h->R, C * K));
     GLST_TRY(dalloc_n(h, &h->part, (size_t)h->nsplit * N));
@@ -322,16 +370,17 @@ static glst_status phase_shell(glst_handle *h, cudaStream_t st) {
 static glst_status phase_lr(glst_handle *h, cudaStream_t st) {
   if (!h->K || !h->plan.natom) return GLST_OK;
   dim3 grid(h->plan.ncell, h->nsplit);
-  dev::k_long_range<<<grid, dev::kLrThreads, 0, st>>>(h->pk, h->cell_count, h->cell_point, h->node32, h->R,
-                                                      h->K, h->nodes_per_split, h->plan.natom, h->part);
+  dev::k_long_range<<<grid, dev::kLrThreads, 0, st>>>(h->pk, h->cell_count, h->cell_point, h->chunks, h->dirs,
+                                                      h->kappa, h->R, h->K, h->plan.natom, h->part);
   CUDA_TRY(cudaGetLastError());
   return GLST_OK;
 }
 
 static glst_status phase_sr(glst_handle *h, cudaStream_t st) {
   if (!h->plan.natom) return GLST_OK;
-  dev::k_short_range<<<h->plan.ncell, dev::kSrThreads, 0, st>>>(h->pd, h->cell_count, h->cell_point,
-                                                                 h->grid, h->sr);
+  dim3 grid(h->plan.ncell, dev::kSrPlanes);
+  dev::k_short_range<<<grid, dev::kSrThreads, 0, st>>>(h->pd, h->cell_count, h->cell_point, h->grid,
+                                                       h->plan.natom, h->sr);
   CUDA_TRY(cudaGetLastError());
   return GLST_OK;
 }

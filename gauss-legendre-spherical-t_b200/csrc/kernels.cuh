@@ -254,9 +254,10 @@ k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ 
 // Shell sums (src/glst_force.cu:702-913 restated for shared memory): per
 // node, an inclusive 3-D prefix sum of S over the cell grid (z, y, x), then
 // R_c = w * [box(c, r_out) - box(c, r_in)], 8 corners per box, clipped to the
-// grid.  All FP64.  Output R'_c(k) = R_c(k) e^{+ik.c} as float2.
-// CTA: nb nodes at once (nb = shared-memory budget / (16 C)), 256 threads.
-constexpr int kSatThreads = 256;
+// grid.  All FP64.  Output R'_c(k) = R_c(k) e^{+ik.c} as float2, the twiddle
+// built from per-axis tables e^{i kx cx} e^{i ky cy} e^{i kz cz}.
+// CTA: nb nodes at once (rows of ncell+1 complex doubles in shared memory).
+constexpr int kSatThreads = 512;
 
 struct SatArgs {
   const double2 *S;
@@ -291,12 +292,32 @@ __device__ __forceinline__ double2 cube_sum(const double2 *row, uint32_t x, uint
   return s;
 }
 
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// Dynamic shared memory: nb rows of `stride` complex (the SAT), then the
+// twiddle tables nb x (nx + ny + nz) complex.
 __global__ void __launch_bounds__(kSatThreads)
 k_shell_sums(Grid g, SatArgs a) {
   extern __shared__ double2 s_sat[];
   const uint32_t k0 = blockIdx.x * a.nb;
   const uint32_t nb = min(a.nb, a.K - k0);
   const uint32_t C = g.ncell;
+  const uint32_t naxis = g.nx + g.ny + g.nz;
+  double2 *s_tw = s_sat + (size_t)a.nb * a.stride;
+  // twiddle tables: e^{i k_a (i + 1/2) l} per node and axis
+  for (uint32_t t = threadIdx.x; t < nb * naxis; t += blockDim.x) {
+    const uint32_t j = t / naxis, r = t % naxis;
+    const double4 nk = a.node64[k0 + j];
+    double kc;
+    if (r < g.nx) kc = nk.x * cell_centre(r, g.l);
+    else if (r < g.nx + g.ny) kc = nk.y * cell_centre(r - g.nx, g.l);
+    else kc = nk.z * cell_centre(r - g.nx - g.ny, g.l);
+    double sn, cs;
+    sincos(kc, &sn, &cs);
+    s_tw[t] = make_double2(cs, sn);
+  }
   // load S[c][k0 .. k0+nb) -> s_sat[j*stride + c]
   for (uint32_t t = threadIdx.x; t < C * nb; t += blockDim.x) {
     const uint32_t c = t / nb, j = t % nb;
@@ -340,68 +361,105 @@ k_shell_sums(Grid g, SatArgs a) {
     const double2 *row = s_sat + j * a.stride;
     const double2 o = cube_sum(row, x, y, z, radii >> 16, g);
     const double2 i = cube_sum(row, x, y, z, radii & 0xffffu, g);
-    const double4 nk = a.node64[k];
-    const double sr = (o.x - i.x) * nk.w, si = (o.y - i.y) * nk.w;
-    double ts, tc;
-    sincos(nk.x * cell_centre(x, g.l) + nk.y * cell_centre(y, g.l) + nk.z * cell_centre(z, g.l), &ts, &tc);
-    a.R[(size_t)c * a.K + k] = make_float2(static_cast<float>(sr * tc - si * ts),
-                                           static_cast<float>(sr * ts + si * tc));
+    const double w = a.node64[k].w;
+    const double2 sh = make_double2((o.x - i.x) * w, (o.y - i.y) * w);
+    const double2 *tw = s_tw + j * naxis;
+    const double2 r = cmul(cmul(sh, tw[x]), cmul(tw[g.nx + y], tw[g.nx + g.ny + z]));
+    a.R[(size_t)c * a.K + k] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
   }
 }
 
 // ----------------------------------------------------------------------------
 // Long-range gather (src/glst_force.cu:983-1135 restated):
 //   en_i = q_i Re sum_k e^{ik.d_i} R'_c(k),   f_i = q_i sum_k Im(...) k
-// CTA = (cell, node split); thread = atom of the cell; nodes staged through
-// shared memory in tiles; FP32 inside a tile, FP64 across tiles.
+// Nodes are held in the order group -> direction -> radial, k = kappa_r s_j,
+// so per atom and direction u = s_j . d_i is formed once and each node costs
+// one multiply, one SFU sin/cos pair and four FMAs:
+//   e += c R'x - s R'y,   g += kappa_r (c R'y + s R'x),   f += g s_j.
+// CTA = (cell, chunk of directions of one group); thread = atom of the cell;
+// the chunk's R' rows are staged through shared memory with cp.async in
+// double-buffered tiles.  FP32 inside a direction, FP64 across directions.
 constexpr int kLrThreads = 128;
-constexpr int kLrTile = 256;
+constexpr int kLrTileNodes = 512;   // nodes per shared tile (whole directions)
+
+struct LrChunk {
+  uint32_t node_begin;   // internal index of (first direction, r = 0)
+  uint32_t dir_begin;    // global direction index of the first direction
+  uint32_t n_dir;        // directions in the chunk
+  uint32_t n_rad;        // radial nodes per direction in this group
+  uint32_t kappa_begin;  // offset of this group's radial table
+  uint32_t pad[3];
+};
+
+__device__ __forceinline__ void lr_stage(float2 *dst, const float2 *__restrict__ src, uint32_t n) {
+  // 8-byte cp.async copies (the tile start is only 8-byte aligned)
+  for (uint32_t t = threadIdx.x; t < n; t += kLrThreads) {
+    const unsigned saddr = static_cast<unsigned>(__cvta_generic_to_shared(dst + t));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(saddr), "l"(src + t) : "memory");
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
 
 __global__ void __launch_bounds__(kLrThreads)
 k_long_range(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_count,
-             const uint32_t *__restrict__ cell_point, const float4 *__restrict__ node32,
-             const float2 *__restrict__ R, uint32_t K, uint32_t nodes_per_split, uint32_t natom,
-             double4 *__restrict__ part) {
-  __shared__ float4 s_k[kLrTile];
-  __shared__ float2 s_r[kLrTile];
+             const uint32_t *__restrict__ cell_point, const LrChunk *__restrict__ chunks,
+             const float4 *__restrict__ dirs, const float *__restrict__ kappa,
+             const float2 *__restrict__ R, uint32_t K, uint32_t natom, double4 *__restrict__ part) {
+  __shared__ float2 s_r[2][kLrTileNodes];
+  __shared__ float s_kappa[kLrTileNodes];
   const uint32_t cell = blockIdx.x;
   const uint32_t cnt = cell_count[cell];
+  if (cnt == 0) return;
   const uint32_t start = cell_point[cell];
-  const uint32_t kb = blockIdx.y * nodes_per_split;
-  const uint32_t ke = min(K, kb + nodes_per_split);
-  const uint32_t nwarps_needed = (cnt + 31) / 32;
+  const LrChunk ch = chunks[blockIdx.y];
+  const uint32_t nr = ch.n_rad;
+  const uint32_t dirs_per_tile = max(1u, kLrTileNodes / nr);
+  const uint32_t ntiles = (ch.n_dir + dirs_per_tile - 1) / dirs_per_tile;
+  for (uint32_t t = threadIdx.x; t < nr; t += kLrThreads) s_kappa[t] = kappa[ch.kappa_begin + t];
+  const float2 *Rc = R + (size_t)cell * K + ch.node_begin;
   for (uint32_t a0 = 0; a0 < cnt; a0 += kLrThreads) {
-    // warps with no atom in this chunk skip the arithmetic but keep staging
     const uint32_t ai = a0 + threadIdx.x;
     const bool active = ai < cnt;
-    const bool warp_live = (a0 / 32 + (threadIdx.x >> 5)) < nwarps_needed;
-    float4 p = active ? pk[start + ai] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const bool warp_live = a0 + (threadIdx.x & ~31u) < cnt;
+    const float4 p = active ? pk[start + ai] : make_float4(0.f, 0.f, 0.f, 0.f);
     double ex = 0.0, ey = 0.0, ez = 0.0, ee = 0.0;
-    for (uint32_t t0 = kb; t0 < ke; t0 += kLrTile) {
-      const uint32_t nt = min((uint32_t)kLrTile, ke - t0);
-      __syncthreads();
-      for (uint32_t t = threadIdx.x; t < nt; t += kLrThreads) {
-        s_k[t] = node32[t0 + t];
-        s_r[t] = R[(size_t)cell * K + t0 + t];
+    __syncthreads();
+    lr_stage(s_r[0], Rc, min(dirs_per_tile, ch.n_dir) * nr);
+    for (uint32_t tile = 0; tile < ntiles; tile++) {
+      const uint32_t d0 = tile * dirs_per_tile;
+      const uint32_t nd = min(dirs_per_tile, ch.n_dir - d0);
+      if (tile + 1 < ntiles) {
+        const uint32_t d1 = d0 + dirs_per_tile;
+        lr_stage(s_r[(tile + 1) & 1], Rc + (size_t)d1 * nr, min(dirs_per_tile, ch.n_dir - d1) * nr);
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+      } else {
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
       }
       __syncthreads();
-      if (!warp_live) continue;
-      float fx = 0.f, fy = 0.f, fz = 0.f, fe = 0.f;
+      if (warp_live) {
+        const float2 *tr = s_r[tile & 1];
+        for (uint32_t d = 0; d < nd; d++) {
+          const float4 sj = dirs[ch.dir_begin + d0 + d];
+          const float u = fmaf(sj.x, p.x, fmaf(sj.y, p.y, sj.z * p.z));
+          float e = 0.f, gsum = 0.f;
+          const float2 *rr = tr + d * nr;
 #pragma unroll 4
-      for (uint32_t t = 0; t < nt; t++) {
-        const float4 k = s_k[t];
-        const float2 r = s_r[t];
-        const float th = fmaf(k.x, p.x, fmaf(k.y, p.y, k.z * p.z));
-        float s, c;
-        __sincosf(th, &s, &c);
-        const float dre = fmaf(c, r.x, -s * r.y);
-        const float dim = fmaf(c, r.y, s * r.x);
-        fe += dre;
-        fx = fmaf(dim, k.x, fx);
-        fy = fmaf(dim, k.y, fy);
-        fz = fmaf(dim, k.z, fz);
+          for (uint32_t r = 0; r < nr; r++) {
+            const float2 v = rr[r];
+            const float kap = s_kappa[r];
+            float sn, cs;
+            __sincosf(kap * u, &sn, &cs);
+            e = fmaf(cs, v.x, e);
+            e = fmaf(-sn, v.y, e);
+            gsum = fmaf(kap, fmaf(cs, v.y, sn * v.x), gsum);
+          }
+          ee += e;
+          ex += gsum * sj.x;
+          ey += gsum * sj.y;
+          ez += gsum * sj.z;
+        }
       }
-      ex += fx; ey += fy; ez += fz; ee += fe;
+      __syncthreads();
     }
     if (active) {
       const double q = static_cast<double>(p.w);
@@ -413,31 +471,36 @@ k_long_range(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_co
 // ----------------------------------------------------------------------------
 // Near field (src/glst_force.cu:1170-1544 restated): bare q_i q_j / r over
 // the own cell (self skipped) and the up to 26 neighbour cells inside the
-// grid (open boundary).  FP64 throughout.  CTA per cell, thread per atom.
+// grid (open boundary).  FP64 throughout.  CTA = (cell, neighbour plane
+// dx in {-1, 0, +1}); thread = atom; each plane writes its own partial row,
+// summed by k_combine in a fixed order.
 constexpr int kSrThreads = 128;
+constexpr int kSrPlanes = 3;
 
 __global__ void __launch_bounds__(kSrThreads)
 k_short_range(const double4 *__restrict__ pd, const uint32_t *__restrict__ cell_count,
-              const uint32_t *__restrict__ cell_point, Grid g, double4 *__restrict__ sr) {
+              const uint32_t *__restrict__ cell_point, Grid g, uint32_t natom,
+              double4 *__restrict__ sr) {
   __shared__ double4 s_at[kSrThreads];
   const uint32_t cell = blockIdx.x;
+  const int plane = static_cast<int>(blockIdx.y) - 1;  // dx of the neighbour plane
   const uint32_t cnt = cell_count[cell];
   const uint32_t start = cell_point[cell];
   const int ix = cell / (g.ny * g.nz), iy = (cell / g.nz) % g.ny, iz = cell % g.nz;
+  const int jx = ix + plane;
+  const bool plane_in = jx >= 0 && jx < (int)g.nx;
   for (uint32_t a0 = 0; a0 < cnt; a0 += kSrThreads) {
     const uint32_t ai = a0 + threadIdx.x;
     const bool active = ai < cnt;
     const double4 me = active ? pd[start + ai] : make_double4(0., 0., 0., 0.);
     double fx = 0.0, fy = 0.0, fz = 0.0, en = 0.0;
-    // own cell first, then neighbours in (a, b, c) order as the reference
-    for (int nbi = -1; nbi < 27; nbi++) {
-      int dxc = 0, dyc = 0, dzc = 0;
-      if (nbi >= 0) {
-        if (nbi == 13) continue;  // (0,0,0) handled as nbi == -1
-        dxc = nbi / 9 - 1; dyc = (nbi / 3) % 3 - 1; dzc = nbi % 3 - 1;
-      }
-      const int jx = ix + dxc, jy = iy + dyc, jz = iz + dzc;
-      if (jx < 0 || jy < 0 || jz < 0 || jx >= (int)g.nx || jy >= (int)g.ny || jz >= (int)g.nz) continue;
+    // (own cell first in the dx = 0 plane, as the reference's intra kernel)
+    for (int nbi = 0; nbi < 9 && plane_in; nbi++) {
+      const int o = (plane == 0) ? ((nbi + 4) % 9) : nbi;  // (0,0) first when dx = 0
+      const int dyc = o / 3 - 1, dzc = o % 3 - 1;
+      const int jy = iy + dyc, jz = iz + dzc;
+      if (jy < 0 || jz < 0 || jy >= (int)g.ny || jz >= (int)g.nz) continue;
+      const bool own = plane == 0 && dyc == 0 && dzc == 0;
       const uint32_t nb = (jx * g.ny + jy) * g.nz + jz;
       const uint32_t bcnt = cell_count[nb];
       const uint32_t bstart = cell_point[nb];
@@ -448,12 +511,12 @@ k_short_range(const double4 *__restrict__ pd, const uint32_t *__restrict__ cell_
         __syncthreads();
         if (!active) continue;
         for (uint32_t j = 0; j < nbt; j++) {
-          if (nbi < 0 && b0 + j == ai) continue;  // self
-          const double4 o = s_at[j];
-          const double dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
+          if (own && b0 + j == ai) continue;  // self
+          const double4 o4 = s_at[j];
+          const double dx = me.x - o4.x, dy = me.y - o4.y, dz = me.z - o4.z;
           const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
           const double ir = rsqrt(r2);
-          const double e = me.w * o.w * ir;
+          const double e = me.w * o4.w * ir;
           const double fs = e * ir * ir;
           fx = fma(fs, dx, fx);
           fy = fma(fs, dy, fy);
@@ -462,7 +525,7 @@ k_short_range(const double4 *__restrict__ pd, const uint32_t *__restrict__ cell_
         }
       }
     }
-    if (active) sr[start + ai] = make_double4(fx, fy, fz, en);
+    if (active) sr[(size_t)blockIdx.y * natom + start + ai] = make_double4(fx, fy, fz, en);
   }
 }
 
@@ -488,8 +551,10 @@ k_combine(const double4 *__restrict__ sr, const double4 *__restrict__ part, uint
         acc.x += v.x; acc.y += v.y; acc.z += v.z; acc.w += v.w;
       }
     }
-    const double4 v = sr[p];
-    acc.x += v.x; acc.y += v.y; acc.z += v.z; acc.w += v.w;
+    for (int pl = 0; pl < kSrPlanes; pl++) {
+      const double4 v = sr[(size_t)pl * natom + p];
+      acc.x += v.x; acc.y += v.y; acc.z += v.z; acc.w += v.w;
+    }
     cfx[p] = acc.x; cfy[p] = acc.y; cfz[p] = acc.z; cen[p] = acc.w;
     const uint32_t i = sorted_idx[p];
     if (i < natom) { ofx[i] = acc.x; ofy[i] = acc.y; ofz[i] = acc.z; oen[i] = acc.w; }

@@ -394,6 +394,8 @@ Plan make_plan(uint32_t natom, double tol, const double box[3], double rcut,
     const size_t m = sm->size() / 3;
     g.n_radial = static_cast<unsigned>(xs.size());
     g.n_dir = static_cast<unsigned>(m);
+    g.dirs = *sm;
+    for (size_t i = 0; i < xs.size(); i++) g.kappa.push_back(2.0 * g.alpha * g.zcut * xs[i]);
     const double zc2 = g.zcut * g.zcut;
     for (size_t i = 0; i < xs.size(); i++) {
       for (size_t j = 0; j < m; j++) {

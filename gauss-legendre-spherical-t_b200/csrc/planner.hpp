@@ -41,6 +41,8 @@ struct GroupPlan {
   unsigned r_in = 0, r_out = 0;
   unsigned gl_degree = 0, t_degree = 0;
   unsigned n_radial = 0, n_dir = 0;
+  std::vector<double> kappa;  // radial scales 2 alpha zcut x_i (n_radial)
+  std::vector<double> dirs;   // unit directions s_j, xyz interleaved (3 n_dir)
 };
 
 struct Plan {
