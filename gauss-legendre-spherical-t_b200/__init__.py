@@ -80,6 +80,7 @@ _SIGNATURES = {
     "glst_plan": (_I, [_U32, _D, _D, _D, _D, _D, _I, ctypes.POINTER(GlstInfo), _P, _P, _P, _P, _P]),
     "glst_max_atoms_per_cell": (_U32, []),
     "glst_measure_pipe_peaks": (_I, [_DP, _DP]),
+    "glst_near_field_noalloc": (_I, [_U32, _P, _P, _P, _P, _D, _D, _D, _D, _I, _P, _P, _P, _P, _P]),
     "glst_last_error": (ctypes.c_char_p, []),
     "glst_status_string": (ctypes.c_char_p, [_I]),
     "glst_version": (ctypes.c_char_p, []),

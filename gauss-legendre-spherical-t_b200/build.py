@@ -12,7 +12,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libglst_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", "engine.cu"), os.path.join(HERE, "csrc", "planner.cpp")]
+SOURCES = [os.path.join(HERE, "csrc", "engine.cu"), os.path.join(HERE, "csrc", "planner.cpp"),
+           os.path.join(HERE, "csrc", "noalloc.cu")]
 HEADERS = [os.path.join(HERE, "csrc", "kernels.cuh"), os.path.join(HERE, "csrc", "planner.hpp"),
            os.path.join(ROOT, "include", "glst_c.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -39,6 +39,12 @@ static glst_status fail(glst_status s, const char *fmt, ...) {
   return s;
 }
 
+// For the other translation units of the library: C++ linkage and hidden
+// visibility, so it is not part of the exported interface.
+__attribute__((visibility("hidden"))) void glst_internal_set_last_error(const char *msg) {
+  g_last_error = msg;
+}
+
 #define CUDA_TRY(call)                                                          \
   do {                                                                          \
     cudaError_t e_ = (call);                                                    \

@@ -183,6 +183,36 @@ glst_status glst_check(glst_handle *h, void *stream);
 /* Per-cell atom limit of this build (the cell sort runs in shared memory). */
 uint32_t glst_max_atoms_per_cell(void);
 
+/* Near-field energies and forces WITHOUT ALLOCATING DEVICE MEMORY.  No
+ * counterpart in the reference.  For callers that cannot call cudaMalloc when
+ * they need forces: code that runs while a stream is being captured into a
+ * CUDA graph (allocation is not allowed during capture), and engines or
+ * plugins whose host owns the whole device through its own memory pool.
+ * Computes the reference's near field -- bare Coulomb over the own cell and
+ * the 26 neighbour cells of the grid built from (box, rcut, ct), open
+ * boundary -- which is the complete GLST result when some axis has at most 2
+ * cells (the reference then has no far field, src/glst_force.cu:667-670).
+ * Inputs d_rx..d_qc and outputs d_fx..d_en (input order) are natom device
+ * doubles owned by the caller.  Working memory is one file-scope __device__
+ * array of GLST_NOALLOC_SCRATCH_BYTES, present on every GPU that loads the
+ * library until the process exits; sizes above GLST_NOALLOC_MAX_ATOMS atoms or
+ * GLST_NOALLOC_MAX_CELLS cells return GLST_ERR_SIZE.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress, device
+ * current); make that first call before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU (different streams or devices'
+ * threads racing on one device) corrupt each other; serialise them.  Stream
+ * ordered, does not wait for the GPU.  Cells above the per-cell sort limit
+ * give correct forces in a non-reference within-cell order. */
+#define GLST_NOALLOC_MAX_ATOMS 32768u
+#define GLST_NOALLOC_MAX_CELLS 32768u
+#define GLST_NOALLOC_SCRATCH_BYTES 6554880ull
+glst_status glst_near_field_noalloc(uint32_t natom, const double *d_rx,
+                                    const double *d_ry, const double *d_rz,
+                                    const double *d_qc, double box_x,
+                                    double box_y, double box_z, double rcut,
+                                    glst_ct ct, double *d_fx, double *d_fy,
+                                    double *d_fz, double *d_en, void *stream);
+
 const char *glst_last_error(void);
 const char *glst_status_string(glst_status s);
 const char *glst_version(void);
