@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     return ap.parse_args()
 
 
@@ -164,6 +165,42 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(g, torch, dev, stream, n_steps=4, n_sys=256, seed=0):
+    """256 independent water boxes of uneven size (300-30,000 atoms, two
+    cubature orders): one captured graph over all systems vs the same systems
+    solved one after another (one launch sequence each)."""
+    from glst_b200 import systems
+    sy = systems.batch_uneven(n_sys, seed=seed)
+    ins = [torch.tensor(np.concatenate([s[k] for s in sy]), dtype=torch.float64, device=dev)
+           for k in ("x", "y", "z", "q")]
+    n = ins[0].numel()
+    outs = [torch.empty(n, dtype=torch.float64, device=dev) for _ in range(4)]
+    t0 = time.perf_counter()
+    b = g.GlstBatch(sy, nstreams=16)
+    t_create = time.perf_counter() - t0
+    res = {}
+    for mode, plain in (("batched", False), ("plain", True)):
+        for _ in range(2):
+            b.compute(*ins, *outs, plain=plain, stream=stream)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n_steps):
+            b.compute(*ins, *outs, plain=plain, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / n_steps
+        res[mode] = {"ms_per_step": ms, "value": n / (ms * 1e-3)}
+    b.close()
+    del ins, outs
+    torch.cuda.empty_cache()
+    return {"workload": "%d uneven water boxes, %d atoms (300-30,000 each), 2 cubature orders" % (n_sys, n),
+            "unit": UNIT, "batched": res["batched"], "plain": res["plain"],
+            "ratio": res["plain"]["ms_per_step"] / res["batched"]["ms_per_step"],
+            "create_s": t_create, "steps": n_steps}
+
+
 def run_ours(args, world, rank, local, dist):
     import torch
     g = __graft_entry__.load_package()
@@ -272,7 +309,10 @@ def run_ours(args, world, rank, local, dist):
         "bound": "sfu", "kernel": dom, "achieved": achieved_sfu / 1e9, "peak": sfu_peak / 1e9,
         "unit": "G sincos-results/s", "frac": achieved_sfu / sfu_peak,
         "peak_source": "measured on this GPU by glst_measure_pipe_peaks (MUFU sin+cos loop)",
-        "traffic": None, "pairs_per_launch": pairs,
+        "traffic": 3.191e8 if dom == "long_range" else 5.003e8,
+        "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of this "
+                          "kernel on this workload (profiles/water10k_solve_kernels.md)",
+        "pairs_per_launch": pairs,
         "fp32_fma_peak_per_s": fma_peak,
     }
 
@@ -293,6 +333,8 @@ def run_ours(args, world, rank, local, dist):
         "roofline": roofline,
         "wall_s_timed": wall,
     }
+    if not args.no_batch:
+        line["batched_vs_plain"] = run_batch(g, torch, dev, stream, n_steps=max(2, args.steps // 5))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline_run(sysd)
         line["cpu_baseline"] = {"value": n / cb["seconds_per_solve"], "unit": UNIT, "cores": cb["cores"],

@@ -23,7 +23,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libglst_b200.so")
 TDESIGN_STORE = os.path.join(_HERE, "data", "tdesigns.bin")
 
-__all__ = ["GlstForce", "GlstError", "load_library", "plan", "LIB_PATH", "TDESIGN_STORE", "set_tdesign_path"]
+__all__ = ["GlstForce", "GlstBatch", "GlstError", "load_library", "plan", "LIB_PATH", "TDESIGN_STORE", "set_tdesign_path"]
 
 
 class GlstError(RuntimeError):
@@ -80,6 +80,11 @@ _SIGNATURES = {
     "glst_plan": (_I, [_U32, _D, _D, _D, _D, _D, _I, ctypes.POINTER(GlstInfo), _P, _P, _P, _P, _P]),
     "glst_max_atoms_per_cell": (_U32, []),
     "glst_measure_pipe_peaks": (_I, [_DP, _DP]),
+    "glst_batch_create": (_I, [ctypes.POINTER(_P), _U32, _P, _P, _P, _P, _I, _U32]),
+    "glst_batch_destroy": (_I, [_P]),
+    "glst_batch_compute": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
+    "glst_batch_energies": (_I, [_P, _P, _P]),
+    "glst_batch_system": (_I, [_P, _U32, ctypes.POINTER(_P)]),
     "glst_near_field_noalloc": (_I, [_U32, _P, _P, _P, _P, _D, _D, _D, _D, _I, _P, _P, _P, _P, _P]),
     "glst_last_error": (ctypes.c_char_p, []),
     "glst_status_string": (ctypes.c_char_p, [_I]),
@@ -286,3 +291,54 @@ class GlstForce:
         arrs = [np.empty(K) for _ in range(4)] + [np.empty(K, dtype=np.uint32)]
         _check(self._lib.glst_get_nodes(self._h, *[a.ctypes.data for a in arrs]))
         return tuple(arrs)
+
+
+class GlstBatch:
+    """Many independent systems solved together (glst_batch_* of the C-ABI).
+
+    systems: sequence of dicts with natom, tol, box (3), rcut.  Inputs and
+    outputs are concatenated in system order (``offsets`` gives the starts).
+    ``compute(..., plain=False)`` runs one captured CUDA graph over all
+    systems; ``plain=True`` solves them one after another (baseline).
+    """
+
+    def __init__(self, systems, ct="double", nstreams=16):
+        self._lib = load_library()
+        self._b = ctypes.c_void_p()
+        n = len(systems)
+        natom = np.array([s["natom"] for s in systems], dtype=np.uint32)
+        tol = np.array([s["tol"] for s in systems], dtype=np.float64)
+        box = np.array([list(s["box"]) for s in systems], dtype=np.float64).reshape(-1)
+        rcut = np.array([s["rcut"] for s in systems], dtype=np.float64)
+        _check(self._lib.glst_batch_create(ctypes.byref(self._b), n, natom.ctypes.data, tol.ctypes.data,
+                                           box.ctypes.data, rcut.ctypes.data, 1 if ct == "float" else 0,
+                                           int(nstreams)))
+        self.nsys = n
+        self.natom = natom
+        self.offsets = np.concatenate([[0], np.cumsum(natom.astype(np.int64))])
+
+    def close(self):
+        if self._b:
+            self._lib.glst_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def compute(self, x, y, z, q, fx, fy, fz, en, plain=False, stream=None):
+        _check(self._lib.glst_batch_compute(self._b, _ptr(x), _ptr(y), _ptr(z), _ptr(q), _ptr(fx), _ptr(fy),
+                                            _ptr(fz), _ptr(en), 1 if plain else 0, _stream(stream)))
+
+    def energies(self, stream=None):
+        e = np.empty(self.nsys)
+        _check(self._lib.glst_batch_energies(self._b, e.ctypes.data, _stream(stream)))
+        return e

@@ -733,3 +733,213 @@ glst_status glst_check(glst_handle *h, void *stream) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- batches
+struct glst_batch {
+  int device = 0;
+  std::vector<glst_handle *> sys;
+  std::vector<uint64_t> off;            // atom offsets (prefix sums)
+  std::vector<uint32_t> order;          // systems, largest estimated cost first
+  std::vector<uint32_t> branch_of;      // branch of each system
+  std::vector<cudaStream_t> branch;
+  std::vector<cudaEvent_t> branch_done;
+  cudaStream_t own = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const void *key[8] = {};
+  double *energies = nullptr;           // device, one per system
+};
+
+static void batch_release(glst_batch *b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  for (auto *h : b->sys) {
+    if (h) {
+      release(h);
+      delete h;
+    }
+  }
+  b->sys.clear();
+  for (auto s : b->branch) cudaStreamDestroy(s);
+  for (auto e : b->branch_done) cudaEventDestroy(e);
+  b->branch.clear();
+  b->branch_done.clear();
+  if (b->own) cudaStreamDestroy(b->own);
+  if (b->ev_in) cudaEventDestroy(b->ev_in);
+  if (b->ev_out) cudaEventDestroy(b->ev_out);
+  if (b->energies) cudaFree(b->energies);
+  b->own = nullptr;
+  b->ev_in = b->ev_out = nullptr;
+  b->energies = nullptr;
+}
+
+// One system: solve, then copy its outputs into the batch's arrays.
+static glst_status batch_one(glst_batch *b, uint32_t i, const double *const in[4], double *const out[4],
+                             cudaStream_t st) {
+  glst_handle *h = b->sys[i];
+  const size_t o = b->off[i], n = h->plan.natom;
+  GLST_TRY(compute_all(h, in[0] + o, in[1] + o, in[2] + o, in[3] + o, st));
+  double *src[4] = {h->ofx, h->ofy, h->ofz, h->oen};
+  for (int k = 0; k < 4; k++)
+    if (n && out[k]) CUDA_TRY(cudaMemcpyAsync(out[k] + o, src[k], n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(b->energies + i, h->energy, sizeof(double), cudaMemcpyDeviceToDevice, st));
+  return GLST_OK;
+}
+
+static glst_status batch_capture(glst_batch *b, const double *const in[4], double *const out[4]) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  CUDA_TRY(cudaStreamBeginCapture(b->own, cudaStreamCaptureModeThreadLocal));
+  glst_status s = GLST_OK;
+  cudaError_t e = cudaEventRecord(b->ev_in, b->own);
+  for (size_t j = 0; e == cudaSuccess && j < b->branch.size(); j++) e = cudaStreamWaitEvent(b->branch[j], b->ev_in, 0);
+  for (size_t t = 0; e == cudaSuccess && s == GLST_OK && t < b->order.size(); t++) {
+    const uint32_t i = b->order[t];
+    s = batch_one(b, i, in, out, b->branch[b->branch_of[i]]);
+  }
+  for (size_t j = 0; e == cudaSuccess && j < b->branch.size(); j++) {
+    e = cudaEventRecord(b->branch_done[j], b->branch[j]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->own, b->branch_done[j], 0);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(b->own, &g);
+  if (s != GLST_OK) {
+    if (g) cudaGraphDestroy(g);
+    return s;
+  }
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return fail(GLST_ERR_CUDA, "batch graph capture failed: %s",
+                cudaGetErrorString(e != cudaSuccess ? e : e2));
+  }
+  b->graph = g;
+  CUDA_TRY(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  for (int k = 0; k < 4; k++) {
+    b->key[k] = in[k];
+    b->key[4 + k] = out[k];
+  }
+  return GLST_OK;
+}
+
+extern "C" {
+
+glst_status glst_batch_create(glst_batch **out, uint32_t nsys, const uint32_t *natom, const double *tol,
+                              const double *box, const double *rcut, glst_ct ct, uint32_t nstreams) {
+  if (!out || (nsys && (!natom || !tol || !box || !rcut)))
+    return fail(GLST_ERR_INVALID_ARG, "null argument");
+  if (ct != GLST_CT_DOUBLE && ct != GLST_CT_FLOAT) return fail(GLST_ERR_INVALID_ARG, "bad calculation type");
+  *out = nullptr;
+  auto b = std::make_unique<glst_batch>();
+  CUDA_TRY(cudaGetDevice(&b->device));
+  std::vector<double> cost(nsys);
+  uint64_t acc = 0;
+  for (uint32_t i = 0; i < nsys; i++) {
+    auto h = std::make_unique<glst_handle>();
+    const double bx[3] = {box[3 * i], box[3 * i + 1], box[3 * i + 2]};
+    glst_status s = setup(h.get(), natom[i], tol[i], bx, rcut[i], ct == GLST_CT_FLOAT);
+    if (s != GLST_OK) {
+      release(h.get());
+      batch_release(b.get());
+      return s;
+    }
+    b->off.push_back(acc);
+    acc += natom[i];
+    // cost model: far-field pairs plus near-field pairs (~ N * 27 * N/C)
+    const double N = natom[i], C = h->plan.ncell;
+    cost[i] = N * (double)h->K + N * 27.0 * N / C * 4.0 + 2e5;
+    b->sys.push_back(h.release());
+  }
+  b->off.push_back(acc);
+  const uint32_t ns = std::max<uint32_t>(1, std::min<uint32_t>(nstreams ? nstreams : 16, std::max<uint32_t>(1, nsys)));
+  for (uint32_t j = 0; j < ns; j++) {
+    cudaStream_t st;
+    cudaEvent_t ev;
+    CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    b->branch.push_back(st);
+    b->branch_done.push_back(ev);
+  }
+  // largest first onto the least loaded branch
+  b->order.resize(nsys);
+  for (uint32_t i = 0; i < nsys; i++) b->order[i] = i;
+  std::stable_sort(b->order.begin(), b->order.end(), [&](uint32_t a, uint32_t c) { return cost[a] > cost[c]; });
+  std::vector<double> load(ns, 0.0);
+  b->branch_of.assign(nsys, 0);
+  for (uint32_t i : b->order) {
+    const uint32_t j = (uint32_t)(std::min_element(load.begin(), load.end()) - load.begin());
+    b->branch_of[i] = j;
+    load[j] += cost[i];
+  }
+  CUDA_TRY(cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking));
+  CUDA_TRY(cudaEventCreateWithFlags(&b->ev_in, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&b->ev_out, cudaEventDisableTiming));
+  CUDA_TRY(cudaMalloc(&b->energies, sizeof(double) * std::max<uint32_t>(1, nsys)));
+  CUDA_TRY(cudaMemset(b->energies, 0, sizeof(double) * std::max<uint32_t>(1, nsys)));
+  *out = b.release();
+  return GLST_OK;
+}
+
+glst_status glst_batch_destroy(glst_batch *b) {
+  if (!b) return GLST_OK;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(b->device);
+  cudaDeviceSynchronize();
+  batch_release(b);
+  delete b;
+  if (prev >= 0) cudaSetDevice(prev);
+  return GLST_OK;
+}
+
+glst_status glst_batch_compute(glst_batch *b, const double *rx, const double *ry, const double *rz,
+                               const double *qc, double *fx, double *fy, double *fz, double *en, int plain,
+                               void *stream) {
+  if (!b) return fail(GLST_ERR_INVALID_ARG, "null batch");
+  if (b->off.back() && (!rx || !ry || !rz || !qc)) return fail(GLST_ERR_INVALID_ARG, "null input pointer");
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != b->device) cudaSetDevice(b->device);
+  struct Restore {
+    int d;
+    ~Restore() {
+      if (d >= 0) cudaSetDevice(d);
+    }
+  } restore{prev != b->device ? prev : -1};
+  const double *in[4] = {rx, ry, rz, qc};
+  double *out[4] = {fx, fy, fz, en};
+  cudaStream_t st = S_(stream);
+  if (plain) {
+    for (uint32_t i = 0; i < b->sys.size(); i++) GLST_TRY(batch_one(b, i, in, out, st));
+    return GLST_OK;
+  }
+  bool same = b->exec != nullptr;
+  for (int k = 0; k < 4 && same; k++) same = b->key[k] == in[k] && b->key[4 + k] == out[k];
+  if (!same) GLST_TRY(batch_capture(b, in, out));
+  CUDA_TRY(cudaEventRecord(b->ev_in, st));
+  CUDA_TRY(cudaStreamWaitEvent(b->own, b->ev_in, 0));
+  CUDA_TRY(cudaGraphLaunch(b->exec, b->own));
+  CUDA_TRY(cudaEventRecord(b->ev_out, b->own));
+  CUDA_TRY(cudaStreamWaitEvent(st, b->ev_out, 0));
+  return GLST_OK;
+}
+
+glst_status glst_batch_energies(glst_batch *b, double *e, void *stream) {
+  if (!b || !e) return fail(GLST_ERR_INVALID_ARG, "null argument");
+  if (b->sys.empty()) return GLST_OK;
+  CUDA_TRY(cudaMemcpyAsync(e, b->energies, b->sys.size() * sizeof(double), cudaMemcpyDeviceToHost, S_(stream)));
+  CUDA_TRY(cudaStreamSynchronize(S_(stream)));
+  return GLST_OK;
+}
+
+glst_status glst_batch_system(glst_batch *b, uint32_t i, glst_handle **h) {
+  if (!b || !h || i >= b->sys.size()) return fail(GLST_ERR_INVALID_ARG, "bad batch index");
+  *h = b->sys[i];
+  return GLST_OK;
+}
+
+}  // extern "C"

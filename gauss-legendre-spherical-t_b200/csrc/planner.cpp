@@ -11,7 +11,9 @@
 #include <dirent.h>
 #include <fstream>
 #include <limits>
+#include <mutex>
 #include <sys/stat.h>
+#include <tuple>
 
 #include "glst_c.h"
 
@@ -304,6 +306,20 @@ static unsigned select_tdesign(const std::vector<double> *&design,
   return t_last;
 }
 
+struct PlanKey {
+  double tol;
+  int ct_float;
+  uint32_t n[3];
+  double cell_dim;
+  const TDesignStore *store;
+  bool operator<(const PlanKey &o) const {
+    return std::tie(tol, ct_float, n[0], n[1], n[2], cell_dim, store) <
+           std::tie(o.tol, o.ct_float, o.n[0], o.n[1], o.n[2], o.cell_dim, o.store);
+  }
+};
+static std::mutex g_plan_mu;
+static std::map<PlanKey, Plan> g_plan_cache;
+
 double rcut_from_ncell(const double box[3], const uint32_t ncell[3]) {
   // rcut = min(L/n) (src/glst_force.cu:80-95).
   const double rx = box[0] / static_cast<double>(ncell[0]);
@@ -350,6 +366,24 @@ Plan make_plan(uint32_t natom, double tol, const double box[3], double rcut,
     throw PlanError{GLST_ERR_SIZE, "cell grid too large"};
   p.ncell = static_cast<uint32_t>(nc);
   p.has_far = p.n[0] > 2 && p.n[1] > 2 && p.n[2] > 2;
+
+  // The groups and the cubature depend only on (tol, CT, grid, cell edge,
+  // t-design source), not on natom or the exact box: reuse earlier plans.
+  PlanKey key{tol, ct_float, {p.n[0], p.n[1], p.n[2]}, p.cell_dim, &store};
+  {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    auto it = g_plan_cache.find(key);
+    if (it != g_plan_cache.end()) {
+      const Plan &c = it->second;
+      p.groups = c.groups;
+      p.kx = c.kx;
+      p.ky = c.ky;
+      p.kz = c.kz;
+      p.w = c.w;
+      p.group = c.group;
+      return p;
+    }
+  }
 
   // Alpha groups (src/glst_force.cu:1643-1724).  Cells are cubes, so the
   // reference's lmin and lmax are both the cell edge.
@@ -411,6 +445,11 @@ Plan make_plan(uint32_t natom, double tol, const double box[3], double rcut,
   }
   if (p.kx.size() > 0xFFFFFFFFull)
     throw PlanError{GLST_ERR_SIZE, "too many cubature nodes"};
+  {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    if (g_plan_cache.size() > 256) g_plan_cache.clear();
+    g_plan_cache.emplace(key, p);
+  }
   return p;
 }
 

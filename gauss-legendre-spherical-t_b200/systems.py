@@ -131,3 +131,24 @@ def read_charmm(prefix):
 def recenter(x, y, z):
     """Shift so the minimum coordinate on each axis is 0 (utils/utils.cpp:35-58)."""
     return x - x.min(), y - y.min(), z - z.min()
+
+
+# ----------------------------------------------------------------- batches
+WATER_DENSITY = 0.0334  # molecules / A^3
+
+
+def batch_uneven(n_sys=256, seed=0, mol_min=100, mol_max=10000, rcut=10.0, alpha=0.31):
+    """Independent water boxes of uneven size: molecule counts log-uniform in
+    [mol_min, mol_max], box edge (n / 0.0334)^(1/3), cutoff rcut, and per
+    system one of two cubature orders, tol = erfc(alpha rcut)/rcut or a
+    tenth of it, drawn uniformly.  Returns a list of system dicts."""
+    rng = np.random.default_rng(seed)
+    t0 = tol_from_alpha(alpha, rcut)
+    out = []
+    for i in range(n_sys):
+        n_mol = int(round(math.exp(rng.uniform(math.log(mol_min), math.log(mol_max)))))
+        L = (n_mol / WATER_DENSITY) ** (1.0 / 3.0)
+        tol = t0 if rng.uniform() < 0.5 else 0.1 * t0
+        x, y, z, q = water_box(n_mol, L, seed=seed * 100003 + i)
+        out.append(dict(x=x, y=y, z=z, q=q, box=(L, L, L), rcut=rcut, tol=tol, natom=len(x)))
+    return out

@@ -183,6 +183,41 @@ glst_status glst_check(glst_handle *h, void *stream);
 /* Per-cell atom limit of this build (the cell sort runs in shared memory). */
 uint32_t glst_max_atoms_per_cell(void);
 
+/* ---------------------------------------------------------------------------
+ * Batches: many independent systems solved together.  No counterpart in the
+ * reference (one system per glst_force object).  Each system keeps its own
+ * plan and buffers; one compute runs all of them as one CUDA graph whose
+ * branches (nstreams concurrent streams, systems assigned largest-first) fill
+ * the GPU with systems of uneven size.  Inputs/outputs are concatenated in
+ * system order: system i owns entries [off_i, off_i + natom_i), off_i the
+ * prefix sum of natom.
+ * ------------------------------------------------------------------------- */
+typedef struct glst_batch glst_batch;
+
+glst_status glst_batch_create(glst_batch **out, uint32_t nsys,
+                              const uint32_t *natom, const double *tol,
+                              const double *box /* 3 per system */,
+                              const double *rcut, glst_ct ct,
+                              uint32_t nstreams);
+glst_status glst_batch_destroy(glst_batch *b);
+
+/* Solve every system.  `plain` = 0: the captured graph (captured on the first
+ * call and again whenever the pointers change); `plain` = 1: the systems one
+ * after another on one stream, each its own launch sequence (the
+ * one-system-per-launch baseline).  Outputs in input order per system.
+ * Stream ordered. */
+glst_status glst_batch_compute(glst_batch *b, const double *d_rx,
+                               const double *d_ry, const double *d_rz,
+                               const double *d_qc, double *d_fx, double *d_fy,
+                               double *d_fz, double *d_en, int plain,
+                               void *stream);
+
+/* Total energy of every system (nsys doubles, host), waits for the stream. */
+glst_status glst_batch_energies(glst_batch *b, double *e, void *stream);
+
+/* Handle of system i (owned by the batch; do not destroy). */
+glst_status glst_batch_system(glst_batch *b, uint32_t i, glst_handle **h);
+
 /* Near-field energies and forces WITHOUT ALLOCATING DEVICE MEMORY.  No
  * counterpart in the reference.  For callers that cannot call cudaMalloc when
  * they need forces: code that runs while a stream is being captured into a
