@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
     return ap.parse_args()
 
 
@@ -165,6 +166,21 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def weak_throughput(local_ms, local_atoms, dist=None, device=None):
+    """Whole-job throughput of independent per-rank work: every rank
+    processed `local_atoms` in `local_ms`; the job takes the slowest rank's
+    time (max over ranks) and processed world x local_atoms.  Returns
+    (max_ms, atoms per second)."""
+    world = 1
+    if dist is not None and dist.is_initialized():
+        import torch
+        world = dist.get_world_size()
+        t = torch.tensor([float(local_ms)], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        local_ms = float(t.item())
+    return local_ms, world * local_atoms / (local_ms * 1e-3)
+
+
 def run_batch(g, torch, dev, stream, n_steps=4, n_sys=256, seed=0):
     """256 independent water boxes of uneven size (300-30,000 atoms, two
     cubature orders): one captured graph over all systems vs the same systems
@@ -199,6 +215,50 @@ def run_batch(g, torch, dev, stream, n_steps=4, n_sys=256, seed=0):
             "unit": UNIT, "batched": res["batched"], "plain": res["plain"],
             "ratio": res["plain"]["ms_per_step"] / res["batched"]["ms_per_step"],
             "create_s": t_create, "steps": n_steps}
+
+
+def run_serve(g, n_requests=120, loads=(0.5, 0.8, 1.1), budget=150 << 30, nslots=8, seed=0):
+    """Served request stream: requests of 1,000-200,000 atoms (log-uniform),
+    60 % continuing a resident system with every atom displaced by
+    N(0, 0.01 A); HBM budget 150 GB.  Capacity = requests/s with every
+    request queued at once; then Poisson arrivals at 3 offered loads (fractions
+    of that capacity), continuous batching (8 slots) vs one request at a time
+    (1 slot).  Latency = submit to completion."""
+    from glst_b200 import systems
+    reqs = systems.request_stream(n_requests, seed=seed)
+    atoms = sum(len(r["x"]) for r in reqs)
+
+    def serve(nslots_, arrivals):
+        with g.GlstServer(budget, nslots=nslots_) as srv:
+            tickets = []
+            t0 = time.perf_counter()
+            for r, ta in zip(reqs, arrivals):
+                dt = ta - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                tickets.append(srv.submit(r["key"], r["x"], r["y"], r["z"], r["q"], r["tol"], r["box"], r["rcut"]))
+            lat = [srv.wait(t, timeout_ms=300000)[5] * 1e-3 for t in tickets]
+            span = time.perf_counter() - t0
+            st = srv.stats()
+        lat.sort()
+        return {"p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                "value": atoms / span, "requests_per_s": len(lat) / span,
+                "evictions": int(st.evictions), "systems_created": int(st.systems_created)}
+
+    zero = [0.0] * len(reqs)
+    serve(nslots, zero)  # warm-up pass: plans, pinned staging, first kernel launches
+    cap = serve(nslots, zero)
+    cap_plain = serve(1, zero)
+    rng = np.random.default_rng(seed + 1)
+    out = {"workload": "%d requests, %d atoms, 1,000-200,000 atoms each, 60%% continue a resident system"
+                       % (len(reqs), atoms), "unit": UNIT, "budget_bytes": budget,
+           "capacity": {"continuous_batching": cap, "one_at_a_time": cap_plain}, "loads": []}
+    for f in loads:
+        rate = f * cap["requests_per_s"]
+        arr = np.cumsum(rng.exponential(1.0 / rate, len(reqs))).tolist()
+        out["loads"].append({"offered": f, "rate_per_s": rate, "continuous_batching": serve(nslots, arr),
+                             "one_at_a_time": serve(1, arr)})
+    return out
 
 
 def run_ours(args, world, rank, local, dist):
@@ -260,13 +320,8 @@ def run_ours(args, world, rank, local, dist):
     wall = time.perf_counter() - wall0
     clk = clocks.stop()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms, value = weak_throughput(sum(step_ms), n * args.steps, dist, dev)
     f.check(stream=stream)
-    value = world * n * args.steps / (total_ms * 1e-3)
 
     # end to end through the public API from pinned host memory
     hx = [torch.tensor(sysd[k], dtype=torch.float64).pin_memory() for k in ("x", "y", "z", "q")]
@@ -292,12 +347,7 @@ def run_ours(args, world, rank, local, dist):
         host_step()
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_val = world * n * e_steps / (e2e_ms * 1e-3)
+    e2e_ms, e2e_val = weak_throughput(e0.elapsed_time(e1), n * e_steps, dist, dev)
 
     # roofline of the dominant kernel (SFU-bound phase kernels)
     sfu_peak, fma_peak = g.measure_pipe_peaks()
@@ -333,8 +383,12 @@ def run_ours(args, world, rank, local, dist):
         "roofline": roofline,
         "wall_s_timed": wall,
     }
-    if not args.no_batch:
+    if world == 1 and not args.no_batch:
         line["batched_vs_plain"] = run_batch(g, torch, dev, stream, n_steps=max(2, args.steps // 5))
+    if world == 1 and not args.no_serve:
+        f.close()
+        torch.cuda.empty_cache()
+        line["served"] = run_serve(g)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline_run(sysd)
         line["cpu_baseline"] = {"value": n / cb["seconds_per_solve"], "unit": UNIT, "cores": cb["cores"],

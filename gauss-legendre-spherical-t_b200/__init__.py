@@ -23,7 +23,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libglst_b200.so")
 TDESIGN_STORE = os.path.join(_HERE, "data", "tdesigns.bin")
 
-__all__ = ["GlstForce", "GlstBatch", "GlstError", "load_library", "plan", "LIB_PATH", "TDESIGN_STORE", "set_tdesign_path"]
+__all__ = ["GlstForce", "GlstBatch", "GlstServer", "GlstError", "load_library", "plan", "LIB_PATH", "TDESIGN_STORE", "set_tdesign_path"]
 
 
 class GlstError(RuntimeError):
@@ -59,6 +59,7 @@ _DP = ctypes.POINTER(ctypes.c_double)
 _SIGNATURES = {
     "glst_set_tdesign_path": (_I, [ctypes.c_char_p]),
     "glst_create": (_I, [ctypes.POINTER(_P), _U32, _D, _D, _D, _D, _D, _I]),
+    "glst_create_shard": (_I, [ctypes.POINTER(_P), _U32, _D, _D, _D, _D, _D, _I, _U32, _U32]),
     "glst_create_ncell": (_I, [ctypes.POINTER(_P), _U32, _D, _D, _D, _D, _U32, _U32, _U32, _I]),
     "glst_init": (_I, [_P, _U32, _D, _D, _D, _D, _D]),
     "glst_destroy": (_I, [_P]),
@@ -80,11 +81,19 @@ _SIGNATURES = {
     "glst_plan": (_I, [_U32, _D, _D, _D, _D, _D, _I, ctypes.POINTER(GlstInfo), _P, _P, _P, _P, _P]),
     "glst_max_atoms_per_cell": (_U32, []),
     "glst_measure_pipe_peaks": (_I, [_DP, _DP]),
+    "glst_autotune": (_I, [_P, _P, _P, _P, _P, _P, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
+    "glst_direct_coulomb": (_I, [_U32, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "glst_batch_create": (_I, [ctypes.POINTER(_P), _U32, _P, _P, _P, _P, _I, _U32]),
     "glst_batch_destroy": (_I, [_P]),
     "glst_batch_compute": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
     "glst_batch_energies": (_I, [_P, _P, _P]),
     "glst_batch_system": (_I, [_P, _U32, ctypes.POINTER(_P)]),
+    "glst_server_create": (_I, [ctypes.POINTER(_P), ctypes.c_uint64, _U32]),
+    "glst_server_destroy": (_I, [_P]),
+    "glst_server_submit": (_I, [_P, ctypes.c_uint64, _U32, _D, _D, _D, _D, _D, _P, _P, _P, _P,
+                                ctypes.POINTER(ctypes.c_uint64)]),
+    "glst_server_wait": (_I, [_P, ctypes.c_uint64, _P, _P, _P, _P, _DP, _DP, _D]),
+    "glst_server_get_stats": (_I, [_P, _P]),
     "glst_near_field_noalloc": (_I, [_U32, _P, _P, _P, _P, _D, _D, _D, _D, _I, _P, _P, _P, _P, _P]),
     "glst_last_error": (ctypes.c_char_p, []),
     "glst_status_string": (ctypes.c_char_p, [_I]),
@@ -161,6 +170,13 @@ def plan(natom, tol, box, rcut, ct="double", with_nodes=True):
     return inf, tuple(arrs)
 
 
+def direct_coulomb(x, y, z, q, fx, fy, fz, en, stream=None):
+    """FP64 all-pairs Coulomb on the GPU (device arrays, input order)."""
+    n = x.numel() if hasattr(x, "numel") else len(x)
+    _check(load_library().glst_direct_coulomb(int(n), _ptr(x), _ptr(y), _ptr(z), _ptr(q), _ptr(fx), _ptr(fy),
+                                              _ptr(fz), _ptr(en), _stream(stream)))
+
+
 def measure_pipe_peaks():
     """(MUFU sin+cos results/s, FP32 FMA/s) of the current device."""
     a, b = ctypes.c_double(), ctypes.c_double()
@@ -171,7 +187,8 @@ def measure_pipe_peaks():
 class GlstForce:
     """One GLST system on the current CUDA device (mirrors glst_force<CT>)."""
 
-    def __init__(self, natom, tol, box_dim_x, box_dim_y, box_dim_z, rcut=None, ncell=None, ct="double"):
+    def __init__(self, natom, tol, box_dim_x, box_dim_y, box_dim_z, rcut=None, ncell=None, ct="double",
+                 shard=None):
         self._lib = load_library()
         self._h = ctypes.c_void_p()
         if ct not in ("double", "float"):
@@ -180,7 +197,13 @@ class GlstForce:
         self.ct = ct
         if (rcut is None) == (ncell is None):
             raise ValueError("give exactly one of rcut or ncell")
-        if rcut is not None:
+        if shard is not None:
+            if rcut is None:
+                raise ValueError("a shard needs rcut")
+            s, n = shard
+            _check(self._lib.glst_create_shard(ctypes.byref(self._h), int(natom), float(tol), float(box_dim_x),
+                                               float(box_dim_y), float(box_dim_z), float(rcut), cti, int(s), int(n)))
+        elif rcut is not None:
             _check(self._lib.glst_create(ctypes.byref(self._h), int(natom), float(tol), float(box_dim_x),
                                          float(box_dim_y), float(box_dim_z), float(rcut), cti))
         else:
@@ -217,6 +240,14 @@ class GlstForce:
     # -- compute (src/glst_force.cu:1604-1614 and the six phases) -----------
     def calc_ener_force(self, d_rx, d_ry, d_rz, d_qc, stream=None):
         _check(self._lib.glst_compute(self._h, _ptr(d_rx), _ptr(d_ry), _ptr(d_rz), _ptr(d_qc), _stream(stream)))
+
+    def autotune(self, d_rx, d_ry, d_rz, d_qc, stream=None):
+        """Pick the shell-sum and long-range launch shapes by timing them on
+        these inputs; returns (nodes per shell CTA, long-range waves)."""
+        a, b = ctypes.c_uint32(), ctypes.c_uint32()
+        _check(self._lib.glst_autotune(self._h, _ptr(d_rx), _ptr(d_ry), _ptr(d_rz), _ptr(d_qc), _stream(stream),
+                                       ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
 
     def assign_atoms(self, d_rx, d_ry, d_rz, d_qc, stream=None):
         _check(self._lib.glst_assign_atoms(self._h, _ptr(d_rx), _ptr(d_ry), _ptr(d_rz), _ptr(d_qc),
@@ -342,3 +373,62 @@ class GlstBatch:
         e = np.empty(self.nsys)
         _check(self._lib.glst_batch_energies(self._b, e.ctypes.data, _stream(stream)))
         return e
+
+
+class GlstServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("evictions", ctypes.c_uint64),
+                ("systems_created", ctypes.c_uint64), ("resident_bytes", ctypes.c_uint64),
+                ("peak_resident_bytes", ctypes.c_uint64), ("resident_systems", ctypes.c_uint32),
+                ("in_flight", ctypes.c_uint32)]
+
+
+class GlstServer:
+    """Continuous-batching request server over the engine (glst_server_*).
+
+    ``submit`` queues an energy+force request (host arrays are copied) and
+    returns a ticket; ``wait`` returns (fx, fy, fz, en, energy, latency_us).
+    ``key`` names a resident system whose plan and buffers are reused when
+    the same key comes back with the same natom, tol, box and rcut."""
+
+    def __init__(self, budget_bytes, nslots=8):
+        self._lib = load_library()
+        self._s = ctypes.c_void_p()
+        _check(self._lib.glst_server_create(ctypes.byref(self._s), int(budget_bytes), int(nslots)))
+
+    def close(self):
+        if self._s:
+            self._lib.glst_server_destroy(self._s)
+            self._s = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, key, x, y, z, q, tol, box, rcut):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, q)]
+        t = ctypes.c_uint64()
+        _check(self._lib.glst_server_submit(self._s, int(key), len(arrs[0]), float(tol), float(box[0]),
+                                            float(box[1]), float(box[2]), float(rcut),
+                                            *[a.ctypes.data for a in arrs], ctypes.byref(t)))
+        return t.value, len(arrs[0])
+
+    def wait(self, ticket, timeout_ms=-1.0):
+        t, n = ticket
+        outs = [np.empty(n) for _ in range(4)]
+        e, lat = ctypes.c_double(), ctypes.c_double()
+        _check(self._lib.glst_server_wait(self._s, t, *[o.ctypes.data for o in outs], ctypes.byref(e),
+                                          ctypes.byref(lat), float(timeout_ms)))
+        return (*outs, e.value, lat.value)
+
+    def stats(self):
+        st = GlstServerStats()
+        _check(self._lib.glst_server_get_stats(self._s, ctypes.byref(st)))
+        return st

@@ -111,6 +111,15 @@ struct glst_handle {
   dev::Grid grid{};
   uint32_t K = 0;
   uint32_t nsplit = 1;  // long-range chunks (rows of part)
+  uint32_t shard = 0, nshards = 1;  // node split across devices (1 = whole system)
+  uint32_t k_begin = 0;             // first node (internal order) of this shard
+  uint32_t lr_waves = 8;            // long-range CTAs ~ lr_waves x resident slots
+  size_t part_cap = 0;              // rows the part buffer holds
+  size_t chunk_bytes = 0;
+  size_t sat_per_node = 0;          // shell-sum shared bytes per node
+  size_t sat_budget = 0;            // shell-sum shared bytes per CTA, at most
+  int nsm = 148;
+  std::vector<uint32_t> g_node_base, g_dir_base, g_kappa_base;  // per group, internal order
   uint32_t sat_nb = 1, sat_stride = 0;
   size_t sat_smem = 0;
   uint32_t combine_blocks = 1;
@@ -168,6 +177,11 @@ static glst_status dalloc_n(glst_handle *h, T **out, size_t n) {
 static void release(glst_handle *h) {
   for (auto &b : h->bufs) cudaFree(b.p);
   h->bufs.clear();
+  if (h->chunks) cudaFree(h->chunks);
+  if (h->part) cudaFree(h->part);
+  h->chunks = nullptr;
+  h->part = nullptr;
+  h->part_cap = 0;
   h->bytes = 0;
   if (h->side) cudaStreamDestroy(h->side);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
@@ -176,8 +190,103 @@ static void release(glst_handle *h) {
   h->ev_fork = h->ev_join = nullptr;
 }
 
+// ---------------------------------------------------------------- tuning
+// Launch shapes picked by glst_autotune, remembered per (cells, nodes, atoms
+// bucket) for every later handle of that shape in this process.
+struct Tuning {
+  uint32_t sat_nb = 0, lr_waves = 0;  // 0 = default
+};
+static std::mutex g_tune_mu;
+static std::map<std::tuple<uint32_t, uint32_t, uint32_t>, Tuning> g_tune;
+
+static std::tuple<uint32_t, uint32_t, uint32_t> tune_key(const Plan &p, uint32_t K) {
+  uint32_t nb = 0;
+  for (uint32_t n = p.natom; n > 1; n >>= 1) nb++;  // atoms bucket: log2
+  return std::make_tuple(p.ncell, K, nb);
+}
+
+static Tuning tuned(const Plan &p, uint32_t K) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(tune_key(p, K));
+  return it == g_tune.end() ? Tuning{} : it->second;
+}
+
+// Long-range chunks: whole directions of one group each, sized so that
+// ncell x chunks is about lr_waves waves of resident CTAs; then this
+// device's share when the system is split over several devices.
+static glst_status build_chunks(glst_handle *h) {
+  const Plan &p = h->plan;
+  const size_t C = p.ncell, K = p.has_far ? p.K() : 0, N = p.natom;
+  const size_t slots = (size_t)h->nsm * 16;
+  const size_t want_chunks = std::max<size_t>(1, ((size_t)h->lr_waves * slots + C - 1) / C);
+  const size_t target_nodes = std::max<size_t>(1, K / want_chunks);
+  std::vector<dev::LrChunk> chunks;
+  for (size_t gi = 0; gi < p.groups.size(); gi++) {
+    const auto &g = p.groups[gi];
+    const uint32_t dpc = (uint32_t)std::max<size_t>(1, target_nodes / g.n_radial);
+    for (uint32_t j0 = 0; j0 < g.n_dir; j0 += dpc) {
+      dev::LrChunk c{};
+      c.n_dir = std::min(dpc, g.n_dir - j0);
+      c.n_rad = g.n_radial;
+      c.node_begin = h->g_node_base[gi] + j0 * g.n_radial;
+      c.dir_begin = h->g_dir_base[gi] + j0;
+      c.kappa_begin = h->g_kappa_base[gi];
+      chunks.push_back(c);
+    }
+  }
+  if (h->nshards > 1) {
+    // This device's share of the nodes: a contiguous run of chunks holding
+    // about K/nshards nodes (the reference splits its node list into
+    // contiguous per-GPU ranges, src/glst_force.cu:276-293).
+    std::vector<dev::LrChunk> mine;
+    uint32_t kb = 0, ke = 0;
+    for (const auto &c : chunks) {
+      const uint64_t mid = (uint64_t)c.node_begin + (uint64_t)c.n_dir * c.n_rad / 2;
+      if (mid * h->nshards / K == h->shard) {
+        if (mine.empty()) kb = c.node_begin;
+        ke = c.node_begin + c.n_dir * c.n_rad;
+        mine.push_back(c);
+      }
+    }
+    for (auto &c : mine) c.node_begin -= kb;
+    chunks.swap(mine);
+    h->k_begin = kb;
+    h->K = ke - kb;
+  }
+  if (chunks.size() > 65535) return fail(GLST_ERR_SIZE, "too many long-range chunks");
+  h->nsplit = (uint32_t)chunks.size();
+  if (h->chunks) {
+    cudaFree(h->chunks);
+    h->bytes -= h->chunk_bytes;
+  }
+  h->chunks = nullptr;
+  h->chunk_bytes = 0;
+  if (!chunks.empty()) {
+    h->chunk_bytes = chunks.size() * sizeof(dev::LrChunk);
+    CUDA_TRY(cudaMalloc(&h->chunks, h->chunk_bytes));
+    h->bytes += h->chunk_bytes;
+    CUDA_TRY(cudaMemcpy(h->chunks, chunks.data(), h->chunk_bytes, cudaMemcpyHostToDevice));
+  }
+  if ((size_t)h->nsplit > h->part_cap) {
+    if (h->part) {
+      cudaFree(h->part);
+      h->bytes -= h->part_cap * N * sizeof(double4);
+    }
+    h->part = nullptr;
+    h->part_cap = 0;
+    CUDA_TRY(cudaMalloc(&h->part, std::max<size_t>(1, (size_t)h->nsplit * N) * sizeof(double4)));
+    h->part_cap = h->nsplit;
+    h->bytes += h->part_cap * N * sizeof(double4);
+  }
+  return GLST_OK;
+}
+
 static glst_status setup(glst_handle *h, uint32_t natom, double tol,
-                         const double box[3], double rcut, int ct_float) {
+                         const double box[3], double rcut, int ct_float,
+                         uint32_t shard = 0, uint32_t nshards = 1) {
+  if (nshards == 0 || shard >= nshards) return fail(GLST_ERR_INVALID_ARG, "shard must be < nshards");
+  h->shard = shard;
+  h->nshards = nshards;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
     cudaGetLastError();
@@ -283,38 +392,30 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
       return fail(GLST_ERR_SIZE,
                   "cell grid of %zu cells exceeds the shell-sum shared-memory limit (%zu cells)",
                   C, budget / sizeof(double2) - 1);
+    h->sat_per_node = per_node;
+    h->sat_budget = budget;
     h->sat_nb = (uint32_t)std::max<size_t>(1, std::min<size_t>(16, (100 * 1024) / per_node));
     h->sat_smem = per_node * h->sat_nb;
     // one process-wide maximum, so handles with different plans coexist
     CUDA_TRY(cudaFuncSetAttribute(dev::k_shell_sums, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)budget));
-    // Long-range chunks: whole directions of one group each, sized so that
-    // ncell x chunks is several waves of resident CTAs.
-    const size_t slots = (size_t)nsm * 16;
-    const size_t want_chunks = std::max<size_t>(1, (8 * slots + C - 1) / C);
-    const size_t target_nodes = std::max<size_t>(1, K / want_chunks);
-    std::vector<dev::LrChunk> chunks;
-    for (size_t gi = 0; gi < p.groups.size(); gi++) {
-      const auto &g = p.groups[gi];
-      const uint32_t dpc = (uint32_t)std::max<size_t>(1, target_nodes / g.n_radial);
-      for (uint32_t j0 = 0; j0 < g.n_dir; j0 += dpc) {
-        dev::LrChunk c{};
-        c.n_dir = std::min(dpc, g.n_dir - j0);
-        c.n_rad = g.n_radial;
-        c.node_begin = node_base[gi] + j0 * g.n_radial;
-        c.dir_begin = dir_base[gi] + j0;
-        c.kappa_begin = kappa_base[gi];
-        chunks.push_back(c);
+    h->nsm = nsm;
+    h->g_node_base = node_base;
+    h->g_dir_base = dir_base;
+    h->g_kappa_base = kappa_base;
+    {
+      const Tuning t = tuned(p, h->K);
+      if (t.sat_nb) {
+        h->sat_nb = std::min<uint32_t>(t.sat_nb, (uint32_t)std::max<size_t>(1, budget / per_node));
+        h->sat_smem = per_node * h->sat_nb;
       }
+      if (t.lr_waves) h->lr_waves = t.lr_waves;
     }
-    if (chunks.size() > 65535) return fail(GLST_ERR_SIZE, "too many long-range chunks");
-    h->nsplit = (uint32_t)chunks.size();
-    GLST_TRY(dalloc_n(h, &h->chunks, chunks.size()));
-    CUDA_TRY(cudaMemcpy(h->chunks, chunks.data(), chunks.size() * sizeof(dev::LrChunk), cudaMemcpyHostToDevice));
-    GLST_TRY(dalloc_n(h, &h->S, C * K));
-    GLST_TRY(dalloc_n(h, &h->R, C * K));
-    GLST_TRY(dalloc_n(h, &h->part, (size_t)h->nsplit * N));
+    GLST_TRY(build_chunks(h));
+    GLST_TRY(dalloc_n(h, &h->S, C * (size_t)h->K));
+    GLST_TRY(dalloc_n(h, &h->R, C * (size_t)h->K));
   }
+  if (shard > 0) CUDA_TRY(cudaMemset(h->sr, 0, (size_t)dev::kSrPlanes * N * sizeof(double4)));
   CUDA_TRY(cudaFuncSetAttribute(dev::k_sort_pack, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(dev::kSortCap * sizeof(uint32_t))));
   CUDA_TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
@@ -359,14 +460,15 @@ static glst_status phase_sf(glst_handle *h, cudaStream_t st) {
   if (cg > 65535) return fail(GLST_ERR_SIZE, "too many cells for the structure-factor grid");
   dim3 grid((h->K + per - 1) / per, cg);
   dev::k_structure_factors<<<grid, dev::kSfThreads, 0, st>>>(h->pk, h->cell_count, h->cell_point, h->grid,
-                                                             h->node32, h->node64, h->K, h->S);
+                                                             h->node32 + h->k_begin, h->node64 + h->k_begin,
+                                                             h->K, h->S);
   CUDA_TRY(cudaGetLastError());
   return GLST_OK;
 }
 
 static glst_status phase_shell(glst_handle *h, cudaStream_t st) {
   if (!h->K || !h->plan.natom) return GLST_OK;
-  dev::SatArgs a{h->S, h->node64, h->node_radii, h->K, h->sat_nb, h->sat_stride, h->R};
+  dev::SatArgs a{h->S, h->node64 + h->k_begin, h->node_radii + h->k_begin, h->K, h->sat_nb, h->sat_stride, h->R};
   const uint32_t nblk = (h->K + h->sat_nb - 1) / h->sat_nb;
   dev::k_shell_sums<<<nblk, dev::kSatThreads, h->sat_smem, st>>>(h->grid, a);
   CUDA_TRY(cudaGetLastError());
@@ -383,7 +485,7 @@ static glst_status phase_lr(glst_handle *h, cudaStream_t st) {
 }
 
 static glst_status phase_sr(glst_handle *h, cudaStream_t st) {
-  if (!h->plan.natom) return GLST_OK;
+  if (!h->plan.natom || h->shard > 0) return GLST_OK;  // shard 0 owns the near field
   dim3 grid(h->plan.ncell, dev::kSrPlanes);
   dev::k_short_range<<<grid, dev::kSrThreads, 0, st>>>(h->pd, h->cell_count, h->cell_point, h->grid,
                                                        h->plan.natom, h->sr);
@@ -483,6 +585,22 @@ glst_status glst_create(glst_handle **out, uint32_t natom, double tol, double bx
   return GLST_OK;
 }
 
+glst_status glst_create_shard(glst_handle **out, uint32_t natom, double tol, double bx, double by,
+                              double bz, double rcut, glst_ct ct, uint32_t shard, uint32_t nshards) {
+  if (!out) return fail(GLST_ERR_INVALID_ARG, "null handle pointer");
+  *out = nullptr;
+  if (ct != GLST_CT_DOUBLE && ct != GLST_CT_FLOAT) return fail(GLST_ERR_INVALID_ARG, "bad calculation type");
+  auto h = std::make_unique<glst_handle>();
+  const double box[3] = {bx, by, bz};
+  glst_status s = setup(h.get(), natom, tol, box, rcut, ct == GLST_CT_FLOAT, shard, nshards);
+  if (s != GLST_OK) {
+    release(h.get());
+    return s;
+  }
+  *out = h.release();
+  return GLST_OK;
+}
+
 glst_status glst_create_ncell(glst_handle **out, uint32_t natom, double tol, double bx, double by,
                               double bz, uint32_t ncx, uint32_t ncy, uint32_t ncz, glst_ct ct) {
   if (!ncx || !ncy || !ncz) return fail(GLST_ERR_INVALID_ARG, "cell counts must be > 0");
@@ -496,10 +614,11 @@ glst_status glst_init(glst_handle *h, uint32_t natom, double tol, double bx, dou
   if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
   DeviceGuard guard_(h);
   const int ct = h->plan.ct_float;
+  const uint32_t shard = h->shard, nshards = h->nshards;
   CUDA_TRY(cudaDeviceSynchronize());
   release(h);
   const double box[3] = {bx, by, bz};
-  return setup(h, natom, tol, box, rcut, ct);
+  return setup(h, natom, tol, box, rcut, ct, shard, nshards);
 }
 
 glst_status glst_destroy(glst_handle *h) {
@@ -680,6 +799,73 @@ glst_status glst_get_nodes(const glst_handle *h, double *kx, double *ky, double 
   if (kz) std::memcpy(kz, p.kz.data(), K * sizeof(double));
   if (w) std::memcpy(w, p.w.data(), K * sizeof(double));
   if (group) std::memcpy(group, p.group.data(), K * sizeof(uint32_t));
+  return GLST_OK;
+}
+
+glst_status glst_autotune(glst_handle *h, const double *rx, const double *ry, const double *rz,
+                          const double *qc, void *stream, uint32_t *sat_nb, uint32_t *lr_waves) {
+  if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  DeviceGuard guard_(h);
+  cudaStream_t st = S_(stream);
+  if (h->K && h->plan.natom && h->nshards == 1) {
+    GLST_TRY(phase_assign(h, rx, ry, rz, qc, st));
+    GLST_TRY(phase_sf(h, st));
+    cudaEvent_t a, b;
+    CUDA_TRY(cudaEventCreate(&a));
+    CUDA_TRY(cudaEventCreate(&b));
+    auto timed = [&](glst_status (*ph)(glst_handle *, cudaStream_t), float *ms) -> glst_status {
+      GLST_TRY(ph(h, st));  // warm
+      CUDA_TRY(cudaEventRecord(a, st));
+      for (int i = 0; i < 3; i++) GLST_TRY(ph(h, st));
+      CUDA_TRY(cudaEventRecord(b, st));
+      CUDA_TRY(cudaEventSynchronize(b));
+      CUDA_TRY(cudaEventElapsedTime(ms, a, b));
+      return GLST_OK;
+    };
+    // shell sums: nodes per CTA
+    uint32_t best_nb = h->sat_nb;
+    float best = 1e30f;
+    for (uint32_t nb : {1u, 2u, 4u, 8u, 16u, 32u}) {
+      if (h->sat_per_node * nb > h->sat_budget) break;
+      h->sat_nb = nb;
+      h->sat_smem = h->sat_per_node * nb;
+      float ms = 0.f;
+      GLST_TRY(timed(phase_shell, &ms));
+      if (ms < best) best = ms, best_nb = nb;
+    }
+    h->sat_nb = best_nb;
+    h->sat_smem = h->sat_per_node * best_nb;
+    GLST_TRY(phase_shell(h, st));
+    // long-range gather: waves of chunk CTAs
+    uint32_t best_w = h->lr_waves;
+    best = 1e30f;
+    for (uint32_t w : {2u, 4u, 8u, 16u, 32u}) {
+      h->lr_waves = w;
+      GLST_TRY(build_chunks(h));
+      float ms = 0.f;
+      GLST_TRY(timed(phase_lr, &ms));
+      if (ms < best) best = ms, best_w = w;
+    }
+    h->lr_waves = best_w;
+    GLST_TRY(build_chunks(h));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[tune_key(h->plan, h->K)] = Tuning{h->sat_nb, h->lr_waves};
+  }
+  if (sat_nb) *sat_nb = h->sat_nb;
+  if (lr_waves) *lr_waves = h->lr_waves;
+  return GLST_OK;
+}
+
+glst_status glst_direct_coulomb(uint32_t natom, const double *rx, const double *ry, const double *rz,
+                                const double *qc, double *fx, double *fy, double *fz, double *en, void *stream) {
+  if (natom && (!rx || !ry || !rz || !qc || !fx || !fy || !fz || !en))
+    return fail(GLST_ERR_INVALID_ARG, "null pointer");
+  if (!natom) return GLST_OK;
+  const uint32_t nb = (natom + dev::kDirectThreads - 1) / dev::kDirectThreads;
+  dev::k_direct_coulomb<<<nb, dev::kDirectThreads, 0, S_(stream)>>>(rx, ry, rz, qc, natom, fx, fy, fz, en);
+  CUDA_TRY(cudaGetLastError());
   return GLST_OK;
 }
 
@@ -939,6 +1125,446 @@ glst_status glst_batch_energies(glst_batch *b, double *e, void *stream) {
 glst_status glst_batch_system(glst_batch *b, uint32_t i, glst_handle **h) {
   if (!b || !h || i >= b->sys.size()) return fail(GLST_ERR_INVALID_ARG, "bad batch index");
   *h = b->sys[i];
+  return GLST_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- request server
+//
+// Continuous batching of independent energy+force requests.  Two threads:
+//   worker  -- completes finished requests, admits queued ones (reserving
+//              device memory against the budget, evicting idle resident
+//              systems least recently used first), launches ready requests
+//              on free stream slots;
+//   builder -- creates the handles (planning + allocation) of admitted
+//              requests that need a new system, off the launch path, so the
+//              GPU keeps working while new systems are set up.
+// A request's life: queued -> building (new system) -> ready -> running -> done.
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+#include <unordered_map>
+
+namespace {
+
+using SrvClock = std::chrono::steady_clock;
+
+struct SrvSystem {
+  uint64_t key = 0;
+  glst_handle *h = nullptr;
+  uint64_t bytes = 0;
+  bool busy = false;
+  uint64_t last_use = 0;
+  uint32_t natom = 0;
+  double tol = 0, box[3] = {0, 0, 0}, rcut = 0;
+};
+
+enum class SrvState { Queued, Building, Ready, Running, Done };
+
+struct SrvRequest {
+  uint64_t ticket = 0, key = 0;
+  uint32_t natom = 0;
+  double tol = 0, box[3] = {0, 0, 0}, rcut = 0;
+  std::vector<double> in, out;
+  double energy = 0.0;
+  SrvClock::time_point t_submit, t_done;
+  SrvState state = SrvState::Queued;
+  glst_status status = GLST_OK;
+  std::string err;
+  SrvSystem *sys = nullptr;
+  uint64_t reserved = 0;  // bytes reserved while its system is being built
+};
+
+struct SrvSlot {
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev = nullptr;
+  double *pin = nullptr;  // 4N inputs, then 4N outputs + energy
+  size_t cap = 0;         // atoms the pinned buffer holds
+  SrvRequest *req = nullptr;
+};
+
+// Device bytes a handle for `p` will hold (an upper bound of setup's sizes).
+uint64_t estimate_bytes(const Plan &p, int nsm) {
+  const uint64_t N = p.natom, C = p.ncell, K = p.has_far ? p.K() : 0;
+  uint64_t b = N * (4 * 4 + 16 + 32 + 32 * dev::kSrPlanes + 8 * 8 + 32) + C * 8 + 4096;
+  if (K) {
+    const uint64_t slots = (uint64_t)nsm * 16;
+    const uint64_t chunks = std::max<uint64_t>(1, (8 * slots + C - 1) / C) + p.groups.size() + 1;
+    b += K * (16 + 32 + 4 + 16 + 4) + C * K * (16 + 8) + chunks * N * 32;
+  }
+  return b + 64 * 16 * 64;  // per-buffer allocation granularity
+}
+
+}  // namespace
+
+struct glst_server {
+  int device = 0, nsm = 148;
+  uint64_t budget = 0;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done, cv_build;
+  std::deque<SrvRequest *> queue;      // queued, building and ready requests, arrival order
+  std::deque<SrvRequest *> to_build;   // requests whose system the builder creates
+  std::unordered_map<uint64_t, SrvRequest *> reqs;
+  std::unordered_map<uint64_t, SrvSystem *> resident;  // named systems
+  std::unordered_map<uint64_t, bool> building_key;      // keys with a system under construction
+  std::vector<SrvSlot> slots;
+  std::vector<double *> old_pinned;    // outgrown staging, freed at destroy
+  std::thread worker, builder;
+  bool stop = false;          // worker: finish what is queued, then exit
+  bool stop_builder = false;  // builder: exit (set after the worker has finished)
+  uint64_t next_ticket = 1, clock = 0;
+  uint64_t reserved = 0;               // bytes promised to systems being built
+  glst_server_stats stats{};
+};
+
+static void srv_drop_system(glst_server *s, SrvSystem *sys) {
+  if (sys->key) s->resident.erase(sys->key);
+  s->stats.resident_bytes -= sys->bytes;
+  s->stats.resident_systems--;
+  release(sys->h);
+  delete sys->h;
+  delete sys;
+}
+
+static void srv_finish(glst_server *s, SrvRequest *r, glst_status st, const char *err) {
+  r->status = st;
+  if (err) r->err = err;
+  r->t_done = SrvClock::now();
+  r->state = SrvState::Done;
+  s->stats.completed++;
+  s->cv_done.notify_all();
+}
+
+// Evict idle named systems, least recently used first, until `need` fits.
+static bool srv_make_room(glst_server *s, uint64_t need) {
+  while (s->stats.resident_bytes + s->reserved + need > s->budget) {
+    SrvSystem *victim = nullptr;
+    for (auto &kv : s->resident)
+      if (!kv.second->busy && (!victim || kv.second->last_use < victim->last_use)) victim = kv.second;
+    if (!victim) return false;
+    srv_drop_system(s, victim);
+    s->stats.evictions++;
+  }
+  return true;
+}
+
+// Admission of a queued request (lock held).  Returns true when the request
+// moved on (ready, building, or finished with an error).
+static bool srv_admit(glst_server *s, SrvRequest *r) {
+  if (r->key) {
+    if (s->building_key.count(r->key)) return false;  // its system is being built
+    auto it = s->resident.find(r->key);
+    if (it != s->resident.end()) {
+      SrvSystem *c = it->second;
+      if (c->busy) return false;  // the previous request of this system still runs
+      const bool same = c->natom == r->natom && c->tol == r->tol && c->rcut == r->rcut && c->box[0] == r->box[0] &&
+                        c->box[1] == r->box[1] && c->box[2] == r->box[2];
+      if (same) {
+        c->busy = true;
+        c->last_use = ++s->clock;
+        r->sys = c;
+        r->state = SrvState::Ready;
+        return true;
+      }
+      srv_drop_system(s, c);
+    }
+  }
+  Plan p;
+  try {
+    auto store = get_store();
+    p = glst::make_plan(r->natom, r->tol, r->box, r->rcut, 0, *store);
+  } catch (const PlanError &e) {
+    srv_finish(s, r, static_cast<glst_status>(e.status), e.msg.c_str());
+    return true;
+  }
+  const uint64_t need = estimate_bytes(p, s->nsm);
+  if (need > s->budget) {
+    srv_finish(s, r, GLST_ERR_OUT_OF_MEMORY, "request larger than the server's memory budget");
+    return true;
+  }
+  if (!srv_make_room(s, need)) return false;  // running requests will free memory
+  s->reserved += need;
+  r->reserved = need;
+  r->state = SrvState::Building;
+  if (r->key) s->building_key[r->key] = true;
+  s->to_build.push_back(r);
+  s->cv_build.notify_one();
+  return true;
+}
+
+static void srv_builder(glst_server *s) {
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (true) {
+    s->cv_build.wait(lk, [&] { return s->stop_builder || !s->to_build.empty(); });
+    if (s->to_build.empty()) {
+      if (s->stop_builder) break;
+      continue;
+    }
+    SrvRequest *r = s->to_build.front();
+    s->to_build.pop_front();
+    lk.unlock();
+    auto h = std::make_unique<glst_handle>();
+    const glst_status st = setup(h.get(), r->natom, r->tol, r->box, r->rcut, 0);
+    const std::string err = st == GLST_OK ? std::string() : g_last_error;
+    if (st != GLST_OK) release(h.get());
+    lk.lock();
+    s->reserved -= r->reserved;
+    r->reserved = 0;
+    if (r->key) s->building_key.erase(r->key);
+    if (st != GLST_OK) {
+      for (auto it = s->queue.begin(); it != s->queue.end(); ++it)
+        if (*it == r) {
+          s->queue.erase(it);
+          break;
+        }
+      srv_finish(s, r, st, err.c_str());
+    } else {
+      auto *sys = new SrvSystem();
+      sys->key = r->key;
+      sys->h = h.release();
+      sys->bytes = sys->h->bytes;
+      sys->natom = r->natom;
+      sys->tol = r->tol;
+      sys->rcut = r->rcut;
+      for (int a = 0; a < 3; a++) sys->box[a] = r->box[a];
+      sys->busy = true;
+      sys->last_use = ++s->clock;
+      s->stats.resident_bytes += sys->bytes;
+      s->stats.peak_resident_bytes = std::max(s->stats.peak_resident_bytes, s->stats.resident_bytes);
+      s->stats.resident_systems++;
+      s->stats.systems_created++;
+      if (r->key) s->resident[r->key] = sys;
+      r->sys = sys;
+      r->state = SrvState::Ready;
+    }
+    s->cv_work.notify_all();
+  }
+}
+
+// Launch a ready request on a free slot (lock held).
+static void srv_launch(glst_server *s, SrvRequest *r, SrvSlot &sl) {
+  SrvSystem *sys = r->sys;
+  const size_t N = r->natom;
+  if (sl.cap < N || !sl.pin) {
+    // grow geometrically; an outgrown buffer is kept until destroy (freeing
+    // pinned memory would synchronise the device mid-stream)
+    if (sl.pin) s->old_pinned.push_back(sl.pin);
+    sl.pin = nullptr;
+    sl.cap = std::max<size_t>({N, 2 * sl.cap, 65536});
+    if (cudaHostAlloc(reinterpret_cast<void **>(&sl.pin), (8 * sl.cap + 1) * sizeof(double), 0) != cudaSuccess) {
+      cudaGetLastError();
+      sl.cap = 0;
+      sys->busy = false;
+      if (!sys->key) srv_drop_system(s, sys);
+      srv_finish(s, r, GLST_ERR_OUT_OF_MEMORY, "pinned staging allocation failed");
+      return;
+    }
+  }
+  glst_handle *h = sys->h;
+  std::memcpy(sl.pin, r->in.data(), 4 * N * sizeof(double));
+  glst_status st = GLST_OK;
+  if (N && cudaMemcpyAsync(h->in_host, sl.pin, 4 * N * sizeof(double), cudaMemcpyHostToDevice, sl.st) != cudaSuccess)
+    st = fail(GLST_ERR_CUDA, "request input copy failed");
+  if (st == GLST_OK)
+    st = compute_all(h, h->in_host, h->in_host + N, h->in_host + 2 * N, h->in_host + 3 * N, sl.st);
+  double *src[4] = {h->ofx, h->ofy, h->ofz, h->oen};
+  for (int k = 0; st == GLST_OK && k < 4; k++)
+    if (N && cudaMemcpyAsync(sl.pin + (4 + k) * N, src[k], N * sizeof(double), cudaMemcpyDeviceToHost, sl.st) !=
+                 cudaSuccess)
+      st = fail(GLST_ERR_CUDA, "request output copy failed");
+  if (st == GLST_OK &&
+      cudaMemcpyAsync(sl.pin + 8 * N, h->energy, sizeof(double), cudaMemcpyDeviceToHost, sl.st) != cudaSuccess)
+    st = fail(GLST_ERR_CUDA, "request energy copy failed");
+  if (st == GLST_OK && cudaEventRecord(sl.ev, sl.st) != cudaSuccess) st = fail(GLST_ERR_CUDA, "event record failed");
+  if (st != GLST_OK) {
+    cudaStreamSynchronize(sl.st);
+    sys->busy = false;
+    if (!sys->key) srv_drop_system(s, sys);
+    srv_finish(s, r, st, g_last_error.c_str());
+    return;
+  }
+  r->state = SrvState::Running;
+  sl.req = r;
+  s->stats.in_flight++;
+}
+
+static void srv_worker(glst_server *s) {
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (true) {
+    bool progress = false;
+    // 1. complete requests whose work finished
+    for (auto &sl : s->slots) {
+      if (!sl.req) continue;
+      const cudaError_t q = cudaEventQuery(sl.ev);
+      if (q == cudaErrorNotReady) continue;
+      SrvRequest *r = sl.req;
+      const size_t N = r->natom;
+      if (q == cudaSuccess) {
+        r->out.assign(sl.pin + 4 * N, sl.pin + 8 * N);
+        r->energy = sl.pin[8 * N];
+      }
+      r->sys->busy = false;
+      if (!r->sys->key) srv_drop_system(s, r->sys);
+      r->sys = nullptr;
+      sl.req = nullptr;
+      s->stats.in_flight--;
+      srv_finish(s, r, q == cudaSuccess ? GLST_OK : GLST_ERR_CUDA,
+                 q == cudaSuccess ? nullptr : cudaGetErrorString(q));
+      progress = true;
+    }
+    // 2. admit queued requests (they keep their place if they cannot start:
+    //    system busy or being built, or memory full), launch ready ones
+    for (auto it = s->queue.begin(); it != s->queue.end();) {
+      SrvRequest *r = *it;
+      if (r->state == SrvState::Queued && srv_admit(s, r)) progress = true;
+      if (r->state == SrvState::Done) {
+        it = s->queue.erase(it);
+        continue;
+      }
+      if (r->state == SrvState::Ready) {
+        SrvSlot *free_slot = nullptr;
+        for (auto &sl : s->slots)
+          if (!sl.req) {
+            free_slot = &sl;
+            break;
+          }
+        if (free_slot) {
+          srv_launch(s, r, *free_slot);
+          it = s->queue.erase(it);
+          progress = true;
+          continue;
+        }
+      }
+      ++it;
+    }
+    if (s->stop && s->queue.empty() && s->stats.in_flight == 0) break;
+    // Sleep, releasing the lock: briefly while GPU work is in flight (its
+    // completion is polled), otherwise until a submit or a finished build
+    // notifies -- unless this pass made progress, which may unblock more.
+    if (s->stats.in_flight)
+      s->cv_work.wait_for(lk, std::chrono::microseconds(20));
+    else if (!progress)
+      s->cv_work.wait_for(lk, std::chrono::milliseconds(5));
+  }
+}
+
+extern "C" {
+
+glst_status glst_server_create(glst_server **out, uint64_t budget_bytes, uint32_t nslots) {
+  if (!out || !budget_bytes) return fail(GLST_ERR_INVALID_ARG, "null output or zero budget");
+  *out = nullptr;
+  auto s = std::make_unique<glst_server>();
+  CUDA_TRY(cudaGetDevice(&s->device));
+  CUDA_TRY(cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, s->device));
+  s->budget = budget_bytes;
+  s->slots.resize(std::max<uint32_t>(1, nslots));
+  for (auto &sl : s->slots) {
+    CUDA_TRY(cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming));
+  }
+  glst_server *raw = s.release();
+  raw->worker = std::thread(srv_worker, raw);
+  raw->builder = std::thread(srv_builder, raw);
+  *out = raw;
+  return GLST_OK;
+}
+
+glst_status glst_server_destroy(glst_server *s) {
+  if (!s) return GLST_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  if (s->worker.joinable()) s->worker.join();  // drains the queue (needs the builder)
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop_builder = true;
+  }
+  s->cv_build.notify_all();
+  if (s->builder.joinable()) s->builder.join();
+  cudaSetDevice(s->device);
+  cudaDeviceSynchronize();
+  std::vector<SrvSystem *> left;
+  for (auto &kv : s->resident) left.push_back(kv.second);
+  for (auto *sys : left) srv_drop_system(s, sys);
+  for (auto &sl : s->slots) {
+    if (sl.pin) cudaFreeHost(sl.pin);
+    cudaStreamDestroy(sl.st);
+    cudaEventDestroy(sl.ev);
+  }
+  for (double *p : s->old_pinned) cudaFreeHost(p);
+  for (auto &kv : s->reqs) delete kv.second;
+  delete s;
+  return GLST_OK;
+}
+
+glst_status glst_server_submit(glst_server *s, uint64_t key, uint32_t natom, double tol, double bx, double by,
+                               double bz, double rcut, const double *rx, const double *ry, const double *rz,
+                               const double *qc, uint64_t *ticket) {
+  if (!s || !ticket || (natom && (!rx || !ry || !rz || !qc))) return fail(GLST_ERR_INVALID_ARG, "null argument");
+  auto r = new SrvRequest();
+  r->key = key;
+  r->natom = natom;
+  r->tol = tol;
+  r->box[0] = bx;
+  r->box[1] = by;
+  r->box[2] = bz;
+  r->rcut = rcut;
+  r->in.resize(4ull * natom);
+  const double *src[4] = {rx, ry, rz, qc};
+  for (int k = 0; k < 4; k++)
+    if (natom) std::memcpy(r->in.data() + (size_t)k * natom, src[k], natom * sizeof(double));
+  r->t_submit = SrvClock::now();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) {
+      delete r;
+      return fail(GLST_ERR_STATE, "server is stopping");
+    }
+    r->ticket = s->next_ticket++;
+    s->reqs[r->ticket] = r;
+    s->queue.push_back(r);
+    s->stats.submitted++;
+    *ticket = r->ticket;
+  }
+  s->cv_work.notify_all();
+  return GLST_OK;
+}
+
+glst_status glst_server_wait(glst_server *s, uint64_t ticket, double *fx, double *fy, double *fz, double *en,
+                             double *energy, double *latency_us, double timeout_ms) {
+  if (!s) return fail(GLST_ERR_INVALID_ARG, "null server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) return fail(GLST_ERR_INVALID_ARG, "unknown ticket");
+  SrvRequest *r = it->second;
+  auto ready = [&] { return r->state == SrvState::Done; };
+  if (timeout_ms < 0)
+    s->cv_done.wait(lk, ready);
+  else if (!s->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), ready))
+    return fail(GLST_ERR_STATE, "request not finished within the timeout");
+  s->reqs.erase(it);
+  lk.unlock();
+  std::unique_ptr<SrvRequest> own(r);
+  if (r->status != GLST_OK) return fail(r->status, "%s", r->err.c_str());
+  const size_t N = r->natom;
+  double *dst[4] = {fx, fy, fz, en};
+  for (int k = 0; k < 4; k++)
+    if (dst[k] && N) std::memcpy(dst[k], r->out.data() + (size_t)k * N, N * sizeof(double));
+  if (energy) *energy = r->energy;
+  if (latency_us) *latency_us = std::chrono::duration<double, std::micro>(r->t_done - r->t_submit).count();
+  return GLST_OK;
+}
+
+glst_status glst_server_get_stats(glst_server *s, glst_server_stats *st) {
+  if (!s || !st) return fail(GLST_ERR_INVALID_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  *st = s->stats;
   return GLST_OK;
 }
 

@@ -377,10 +377,12 @@ k_shell_sums(Grid g, SatArgs a) {
 // one multiply, one SFU sin/cos pair and four FMAs:
 //   e += c R'x - s R'y,   g += kappa_r (c R'y + s R'x),   f += g s_j.
 // CTA = (cell, chunk of directions of one group); thread = atom of the cell;
-// the chunk's R' rows are staged through shared memory with cp.async in
-// double-buffered tiles.  FP32 inside a direction, FP64 across directions.
+// the chunk's R' rows are prefetched into registers and staged through
+// double-buffered shared-memory tiles as (R'x, R'y, kappa_r) float4s.  FP32
+// inside a tile (at most 512 nodes), FP64 across tiles.
 constexpr int kLrThreads = 128;
 constexpr int kLrTileNodes = 512;   // nodes per shared tile (whole directions)
+constexpr int kLrPerThread = kLrTileNodes / kLrThreads;
 
 struct LrChunk {
   uint32_t node_begin;   // internal index of (first direction, r = 0)
@@ -391,21 +393,23 @@ struct LrChunk {
   uint32_t pad[3];
 };
 
-__device__ __forceinline__ void lr_stage(float2 *dst, const float2 *__restrict__ src, uint32_t n) {
-  // 8-byte cp.async copies (the tile start is only 8-byte aligned)
-  for (uint32_t t = threadIdx.x; t < n; t += kLrThreads) {
-    const unsigned saddr = static_cast<unsigned>(__cvta_generic_to_shared(dst + t));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(saddr), "l"(src + t) : "memory");
+// Each thread loads its share of a tile's R' values into registers; stored
+// to shared memory (with kappa interleaved) after the previous tile's work.
+__device__ __forceinline__ void lr_prefetch(float2 (&pre)[kLrPerThread], const float2 *__restrict__ src,
+                                            uint32_t n) {
+#pragma unroll
+  for (int k = 0; k < kLrPerThread; k++) {
+    const uint32_t t = threadIdx.x + k * kLrThreads;
+    pre[k] = t < n ? src[t] : make_float2(0.f, 0.f);
   }
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
 
-__global__ void __launch_bounds__(kLrThreads)
+__global__ void __launch_bounds__(kLrThreads, 12)
 k_long_range(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_count,
              const uint32_t *__restrict__ cell_point, const LrChunk *__restrict__ chunks,
              const float4 *__restrict__ dirs, const float *__restrict__ kappa,
              const float2 *__restrict__ R, uint32_t K, uint32_t natom, double4 *__restrict__ part) {
-  __shared__ float2 s_r[2][kLrTileNodes];
+  __shared__ float4 s_n[2][kLrTileNodes];  // (R'x, R'y, kappa_r, 0) per node
   __shared__ float s_kappa[kLrTileNodes];
   const uint32_t cell = blockIdx.x;
   const uint32_t cnt = cell_count[cell];
@@ -423,43 +427,49 @@ k_long_range(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_co
     const bool warp_live = a0 + (threadIdx.x & ~31u) < cnt;
     const float4 p = active ? pk[start + ai] : make_float4(0.f, 0.f, 0.f, 0.f);
     double ex = 0.0, ey = 0.0, ez = 0.0, ee = 0.0;
-    __syncthreads();
-    lr_stage(s_r[0], Rc, min(dirs_per_tile, ch.n_dir) * nr);
+    float2 pre[kLrPerThread];
+    __syncthreads();  // s_kappa written; previous atom block done with s_n
+    lr_prefetch(pre, Rc, min(dirs_per_tile, ch.n_dir) * nr);
     for (uint32_t tile = 0; tile < ntiles; tile++) {
       const uint32_t d0 = tile * dirs_per_tile;
       const uint32_t nd = min(dirs_per_tile, ch.n_dir - d0);
-      if (tile + 1 < ntiles) {
-        const uint32_t d1 = d0 + dirs_per_tile;
-        lr_stage(s_r[(tile + 1) & 1], Rc + (size_t)d1 * nr, min(dirs_per_tile, ch.n_dir - d1) * nr);
-        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-      } else {
-        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+      float4 *buf = s_n[tile & 1];
+#pragma unroll
+      for (int k = 0; k < kLrPerThread; k++) {
+        const uint32_t t = threadIdx.x + k * kLrThreads;
+        if (t < nd * nr) buf[t] = make_float4(pre[k].x, pre[k].y, s_kappa[t % nr], 0.f);
       }
       __syncthreads();
+      if (tile + 1 < ntiles) {
+        const uint32_t d1 = d0 + dirs_per_tile;
+        lr_prefetch(pre, Rc + (size_t)d1 * nr, min(dirs_per_tile, ch.n_dir - d1) * nr);
+      }
       if (warp_live) {
-        const float2 *tr = s_r[tile & 1];
+        float tx = 0.f, ty = 0.f, tz = 0.f, te = 0.f;
         for (uint32_t d = 0; d < nd; d++) {
           const float4 sj = dirs[ch.dir_begin + d0 + d];
           const float u = fmaf(sj.x, p.x, fmaf(sj.y, p.y, sj.z * p.z));
           float e = 0.f, gsum = 0.f;
-          const float2 *rr = tr + d * nr;
+          const float4 *nn = buf + d * nr;
 #pragma unroll 4
           for (uint32_t r = 0; r < nr; r++) {
-            const float2 v = rr[r];
-            const float kap = s_kappa[r];
+            const float4 v = nn[r];
             float sn, cs;
-            __sincosf(kap * u, &sn, &cs);
+            __sincosf(v.z * u, &sn, &cs);
             e = fmaf(cs, v.x, e);
             e = fmaf(-sn, v.y, e);
-            gsum = fmaf(kap, fmaf(cs, v.y, sn * v.x), gsum);
+            gsum = fmaf(v.z, fmaf(cs, v.y, sn * v.x), gsum);
           }
-          ee += e;
-          ex += gsum * sj.x;
-          ey += gsum * sj.y;
-          ez += gsum * sj.z;
+          te += e;
+          tx = fmaf(gsum, sj.x, tx);
+          ty = fmaf(gsum, sj.y, ty);
+          tz = fmaf(gsum, sj.z, tz);
         }
+        ee += te;
+        ex += tx;
+        ey += ty;
+        ez += tz;
       }
-      __syncthreads();
     }
     if (active) {
       const double q = static_cast<double>(p.w);
@@ -583,6 +593,52 @@ __global__ void k_energy_total(const double *__restrict__ block_energy, uint32_t
     double t = 0.0;
     for (unsigned w = 0; w < (blockDim.x >> 5); w++) t += s_red[w];
     *total = 0.5 * t;
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Direct all-pairs Coulomb, FP64, open boundary (the reference's physics
+// check, utils/coulomb.cu:14-82): thread per atom, the other atoms streamed
+// through shared memory.
+constexpr int kDirectThreads = 128;
+
+__global__ void __launch_bounds__(kDirectThreads)
+k_direct_coulomb(const double *__restrict__ rx, const double *__restrict__ ry, const double *__restrict__ rz,
+                 const double *__restrict__ qc, uint32_t n, double *__restrict__ fx, double *__restrict__ fy,
+                 double *__restrict__ fz, double *__restrict__ en) {
+  __shared__ double4 s_at[kDirectThreads];
+  const uint32_t i = blockIdx.x * kDirectThreads + threadIdx.x;
+  const bool active = i < n;
+  const double xi = active ? rx[i] : 0.0, yi = active ? ry[i] : 0.0, zi = active ? rz[i] : 0.0;
+  const double qi = active ? qc[i] : 0.0;
+  double f0 = 0.0, f1 = 0.0, f2 = 0.0, e0 = 0.0;
+  for (uint32_t j0 = 0; j0 < n; j0 += kDirectThreads) {
+    const uint32_t nj = min((uint32_t)kDirectThreads, n - j0);
+    __syncthreads();
+    if (threadIdx.x < nj) {
+      const uint32_t j = j0 + threadIdx.x;
+      s_at[threadIdx.x] = make_double4(rx[j], ry[j], rz[j], qc[j]);
+    }
+    __syncthreads();
+    if (!active) continue;
+    for (uint32_t k = 0; k < nj; k++) {
+      if (j0 + k == i) continue;
+      const double4 o = s_at[k];
+      const double dx = xi - o.x, dy = yi - o.y, dz = zi - o.z;
+      const double ir = rsqrt(fma(dx, dx, fma(dy, dy, dz * dz)));
+      const double e = qi * o.w * ir;
+      const double fs = e * ir * ir;
+      f0 = fma(fs, dx, f0);
+      f1 = fma(fs, dy, f1);
+      f2 = fma(fs, dz, f2);
+      e0 += e;
+    }
+  }
+  if (active) {
+    fx[i] = f0;
+    fy[i] = f1;
+    fz[i] = f2;
+    en[i] = e0;
   }
 }
 

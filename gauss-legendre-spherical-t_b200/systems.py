@@ -152,3 +152,35 @@ def batch_uneven(n_sys=256, seed=0, mol_min=100, mol_max=10000, rcut=10.0, alpha
         x, y, z, q = water_box(n_mol, L, seed=seed * 100003 + i)
         out.append(dict(x=x, y=y, z=z, q=q, box=(L, L, L), rcut=rcut, tol=tol, natom=len(x)))
     return out
+
+
+def request_stream(n_requests, seed=0, atom_min=1000, atom_max=200000, p_continue=0.6, sigma=0.01,
+                   rcut=10.0, alpha=0.31):
+    """Energy+force requests of a served MD-like workload.  With probability
+    p_continue a request continues a resident system (same key, every atom
+    displaced by N(0, sigma) A); otherwise it opens a new water box with an
+    atom count log-uniform in [atom_min, atom_max].  Returns a list of dicts
+    (key, x, y, z, q, box, rcut, tol)."""
+    rng = np.random.default_rng(seed)
+    tol = tol_from_alpha(alpha, rcut)
+    live = {}
+    out = []
+    next_key = 1
+    for _ in range(n_requests):
+        if live and rng.uniform() < p_continue:
+            key = int(rng.choice(list(live)))
+            st = live[key]
+            st["x"] = st["x"] + rng.normal(0.0, sigma, st["x"].size)
+            st["y"] = st["y"] + rng.normal(0.0, sigma, st["y"].size)
+            st["z"] = st["z"] + rng.normal(0.0, sigma, st["z"].size)
+        else:
+            n_atom = math.exp(rng.uniform(math.log(atom_min), math.log(atom_max)))
+            n_mol = max(1, int(round(n_atom / 3.0)))
+            L = (n_mol / WATER_DENSITY) ** (1.0 / 3.0)
+            x, y, z, q = water_box(n_mol, L, seed=int(rng.integers(1 << 30)))
+            key = next_key
+            next_key += 1
+            st = live[key] = dict(x=x, y=y, z=z, q=q, box=(L, L, L))
+        out.append(dict(key=key, x=st["x"].copy(), y=st["y"].copy(), z=st["z"].copy(), q=st["q"],
+                        box=st["box"], rcut=rcut, tol=tol))
+    return out

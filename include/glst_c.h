@@ -95,6 +95,18 @@ glst_status glst_create_ncell(glst_handle **out, uint32_t natom, double tol,
                               uint32_t ncell_x, uint32_t ncell_y,
                               uint32_t ncell_z, glst_ct ct);
 
+/* One device's share of a system split over several GPUs, the reference's
+ * multi-GPU scheme (src/glst_force.cu:276-293 node split, :1584-1602 reduce):
+ * shard s of n computes the structure factors, shell sums and long-range
+ * gather of a contiguous range of about K/n cubature nodes, and shard 0 also
+ * the near field.  The per-atom outputs of the n shards add up to the full
+ * result; sum them across devices (e.g. ncclAllReduce of fx, fy, fz, en) --
+ * the engine does no communication.  Otherwise as glst_create. */
+glst_status glst_create_shard(glst_handle **out, uint32_t natom, double tol,
+                              double box_x, double box_y, double box_z,
+                              double rcut, glst_ct ct, uint32_t shard,
+                              uint32_t nshards);
+
 /* glst_force::init(natom, tol, Lx, Ly, Lz, rcut)   src/glst_force.cu:179-327 */
 glst_status glst_init(glst_handle *h, uint32_t natom, double tol, double box_x,
                       double box_y, double box_z, double rcut);
@@ -169,6 +181,27 @@ glst_status glst_plan(uint32_t natom, double tol, double box_x, double box_y,
                       double *kx, double *ky, double *kz, double *w,
                       uint32_t *group);
 
+/* Autotuner: times the shell-sum kernel for 1..32 nodes per CTA and the
+ * long-range gather for 2..32 waves of chunk CTAs on these inputs (device
+ * FP64 arrays, as glst_compute), keeps the fastest for this handle, and
+ * remembers them for every later handle of the same shape (cells, nodes,
+ * atom-count bucket) in this process.  Returns the choice.  Waits for the
+ * stream; outputs must be recomputed afterwards.  No reference counterpart. */
+glst_status glst_autotune(glst_handle *h, const double *d_rx,
+                          const double *d_ry, const double *d_rz,
+                          const double *d_qc, void *stream, uint32_t *sat_nb,
+                          uint32_t *lr_waves);
+
+/* Direct all-pairs Coulomb energies and forces in FP64, open boundary: the
+ * reference's physics check (utils/coulomb.cu:14-172, compute_coulomb_cuda),
+ * on the current device.  Device arrays of natom doubles, input order; en
+ * counts each pair from both sides like the GLST outputs.  Stream ordered;
+ * O(natom^2) work, meant for checking systems up to ~1e5 atoms. */
+glst_status glst_direct_coulomb(uint32_t natom, const double *d_rx,
+                                const double *d_ry, const double *d_rz,
+                                const double *d_qc, double *d_fx, double *d_fy,
+                                double *d_fz, double *d_en, void *stream);
+
 /* Measured pipe peaks of the current device, the denominators of the
  * roofline of the phase kernels (which are bound by the SFU sin/cos and FP32
  * pipes, not by tensor cores or HBM): `sfu_per_s` = MUFU sin+cos results per
@@ -217,6 +250,49 @@ glst_status glst_batch_energies(glst_batch *b, double *e, void *stream);
 
 /* Handle of system i (owned by the batch; do not destroy). */
 glst_status glst_batch_system(glst_batch *b, uint32_t i, glst_handle **h);
+
+/* ---------------------------------------------------------------------------
+ * Request server: energy+force requests of independent systems served with
+ * continuous batching.  No counterpart in the reference.  A worker thread
+ * admits queued requests as soon as a stream slot is free and the systems'
+ * device memory fits the budget (idle resident systems are evicted least
+ * recently used first), runs each on its own stream (H2D from pinned
+ * staging, solve, D2H), and completes them as their events fire.  A request
+ * naming a resident system (same key, natom, tol, box, rcut) reuses its plan
+ * and buffers: only positions and charges move.
+ * ------------------------------------------------------------------------- */
+typedef struct glst_server glst_server;
+
+typedef struct glst_server_stats {
+  uint64_t submitted, completed, evictions, systems_created;
+  uint64_t resident_bytes, peak_resident_bytes;
+  uint32_t resident_systems, in_flight;
+} glst_server_stats;
+
+/* budget_bytes: device memory the resident systems may hold; nslots:
+ * requests in flight at once (1 = one request at a time). */
+glst_status glst_server_create(glst_server **out, uint64_t budget_bytes,
+                               uint32_t nslots);
+glst_status glst_server_destroy(glst_server *s);
+
+/* Queue a request; inputs are copied before the call returns.  `key` names
+ * the system (0 = a new, unnamed system, freed after the request).  Returns a
+ * ticket.  Host arrays of natom doubles. */
+glst_status glst_server_submit(glst_server *s, uint64_t key, uint32_t natom,
+                               double tol, double box_x, double box_y,
+                               double box_z, double rcut, const double *rx,
+                               const double *ry, const double *rz,
+                               const double *qc, uint64_t *ticket);
+
+/* Wait for a request (timeout_ms < 0: no limit; returns GLST_ERR_STATE on
+ * timeout), copy its outputs (input order, host, any may be NULL), total
+ * energy and latency (submit to completion, microseconds), and forget it. */
+glst_status glst_server_wait(glst_server *s, uint64_t ticket, double *fx,
+                             double *fy, double *fz, double *en,
+                             double *energy, double *latency_us,
+                             double timeout_ms);
+
+glst_status glst_server_get_stats(glst_server *s, glst_server_stats *st);
 
 /* Near-field energies and forces WITHOUT ALLOCATING DEVICE MEMORY.  No
  * counterpart in the reference.  For callers that cannot call cudaMalloc when

@@ -38,7 +38,12 @@ CASES = {
     "w1000_tol1e-4": (1000, 31.04, 8.0, 1e-4, 3),
     "w2000_tol1e-5": (2000, 39.1, 10.0, 1e-5, 5),
     "water10k": (10000, 66.9, 10.0, math.erfc(0.31 * 10.0) / 10.0, 0),
+    # one million atoms; stored as a seeded subset of atoms plus
+    # digests of the full assignment (the full arrays would be 36 MB)
+    "water333k": (333333, 215.3, 10.0, math.erfc(0.31 * 10.0) / 10.0, 0),
 }
+SUBSET = {"water333k": 20000}
+CASE_CTS = {"water333k": ("double",)}
 CTS = ("double", "float")
 
 
@@ -47,6 +52,13 @@ def input_sha256(x, y, z, q):
     same positions and charges the fixture was made from."""
     import hashlib
     return hashlib.sha256(b"".join(np.ascontiguousarray(a, dtype="<f8").tobytes() for a in (x, y, z, q))).hexdigest()
+
+
+def assignment_sha256(sorted_idx, cell_count, cell_point):
+    """Digest of a cell assignment (u32 arrays, little endian)."""
+    import hashlib
+    return hashlib.sha256(b"".join(np.ascontiguousarray(a, dtype="<u4").tobytes()
+                                   for a in (sorted_idx, cell_count, cell_point))).hexdigest()
 
 
 def harness():
@@ -91,7 +103,7 @@ def render_tdesigns(dst):
     make_tdesigns.write_reference_dir(g.TDESIGN_STORE, os.path.join(dst, "SS31-Mar-2016"))
 
 
-def main(cases, iters=5):
+def main(cases, iters=3):
     g = __graft_entry__.load_package()
     from glst_b200 import systems
     if not os.path.exists(harness()):
@@ -105,7 +117,7 @@ def main(cases, iters=5):
             digest = input_sha256(x, y, z, q)
             inp = os.path.join(work, case + ".in")
             write_input(inp, x, y, z, q, tol, L, rcut)
-            for ct in CTS:
+            for ct in CASE_CTS.get(case, CTS):
                 out = os.path.join(work, "%s_%s.out" % (case, ct))
                 r = subprocess.run([harness(), inp, out, ct, str(iters)], cwd=work, capture_output=True,
                                    text=True)
@@ -113,11 +125,21 @@ def main(cases, iters=5):
                     print(r.stdout[-2000:], r.stderr[-2000:])
                     raise SystemExit("reference harness failed on %s/%s (%d)" % (case, ct, r.returncode))
                 o = read_output(out)
-                np.savez_compressed(os.path.join(HERE, "%s_%s.npz" % (case, ct)),
-                                    n_mol=n_mol, box=L, rcut=rcut, tol=tol, seed=seed, K=o["K"],
-                                    ncell=np.array(o["ncell"]), fx=o["fx"], fy=o["fy"], fz=o["fz"], en=o["en"],
-                                    sorted_idx=o["sorted_idx"], cell_count=o["cell_count"],
-                                    cell_point=o["cell_point"], ref_ms=o["ms"], input_sha256=np.array(digest))
+                path = os.path.join(HERE, "%s_%s.npz" % (case, ct))
+                if case in SUBSET:
+                    sel = np.sort(np.random.default_rng(1234).choice(o["natom"], SUBSET[case], replace=False))
+                    np.savez_compressed(path, n_mol=n_mol, box=L, rcut=rcut, tol=tol, seed=seed, K=o["K"],
+                                        ncell=np.array(o["ncell"]), subset=sel, fx=o["fx"][sel], fy=o["fy"][sel],
+                                        fz=o["fz"][sel], en=o["en"][sel], energy_total=0.5 * float(np.sum(o["en"])),
+                                        force_rms=float(np.sqrt(np.mean(o["fx"] ** 2 + o["fy"] ** 2 + o["fz"] ** 2))),
+                                        assignment_sha256=np.array(assignment_sha256(
+                                            o["sorted_idx"], o["cell_count"], o["cell_point"])),
+                                        ref_ms=o["ms"], input_sha256=np.array(digest))
+                else:
+                    np.savez_compressed(path, n_mol=n_mol, box=L, rcut=rcut, tol=tol, seed=seed, K=o["K"],
+                                        ncell=np.array(o["ncell"]), fx=o["fx"], fy=o["fy"], fz=o["fz"], en=o["en"],
+                                        sorted_idx=o["sorted_idx"], cell_count=o["cell_count"],
+                                        cell_point=o["cell_point"], ref_ms=o["ms"], input_sha256=np.array(digest))
                 summary["%s_%s" % (case, ct)] = dict(
                     natom=o["natom"], K=o["K"], ncell=o["ncell"],
                     ms=dict(zip(["assign", "sf", "sum_rmt", "lr", "sr", "comm", "total_host", "total_events"],

@@ -39,6 +39,7 @@ def test_fixtures_present():
     for c in SMALL + ["water10k"]:
         for ct in ("double", "float"):
             assert "%s_%s.npz" % (c, ct) in names
+    assert "water333k_double.npz" in names
 
 
 @pytest.mark.parametrize("case", SMALL)

@@ -39,3 +39,30 @@ def test_cuda_path_matches_reference(pkg, case, ct):
         print(case, ct, rep)
         assert rep["force_rms_rel"] <= FORCE_RMS_TOL, rep
         assert rep["energy_rel"] <= ENERGY_TOL, rep
+
+
+def test_water333k_matches_reference_subset(pkg):
+    """333,333 waters (999,999 atoms), L = 215.3 A.  The fixture
+    holds the reference's outputs on a seeded subset of 20,000 atoms, its
+    total energy, and a digest of its full cell assignment."""
+    import hashlib
+    import os
+    d, (x, y, z, q), box = load_case("water333k", "double")
+    dev = [torch.tensor(a, dtype=torch.float64, device="cuda:0") for a in (x, y, z, q)]
+    with pkg.GlstForce(len(x), float(d["tol"]), *box, rcut=float(d["rcut"])) as f:
+        assert f.info().num_nodes == int(d["K"])
+        f.calc_ener_force(*dev)
+        fx, fy, fz, en = f.get_ef()
+        e = f.energy()
+        sidx, cnt, pnt = f.assignment()
+    digest = hashlib.sha256(b"".join(np.ascontiguousarray(a, dtype="<u4").tobytes()
+                                     for a in (sidx, cnt, pnt))).hexdigest()
+    assert digest == str(d["assignment_sha256"])
+    sel = d["subset"]
+    dF2 = np.sum((fx[sel] - d["fx"]) ** 2 + (fy[sel] - d["fy"]) ** 2 + (fz[sel] - d["fz"]) ** 2)
+    F2 = np.sum(d["fx"] ** 2 + d["fy"] ** 2 + d["fz"] ** 2)
+    rel = float(np.sqrt(dF2 / F2))
+    e_rel = abs(e - float(d["energy_total"])) / abs(float(d["energy_total"]))
+    print("water333k force_rms_rel(subset) %.3e energy_rel %.3e" % (rel, e_rel))
+    assert rel <= FORCE_RMS_TOL
+    assert e_rel <= ENERGY_TOL

@@ -270,3 +270,64 @@ def test_water10k_parity(pkg, store):
     g_sidx, g_cnt, g_pnt = f.assignment()
     assert np.array_equal(g_sidx, sidx) and np.array_equal(g_cnt, cnt) and np.array_equal(g_pnt, pnt)
     f.close()
+
+
+def test_direct_coulomb_kernel_matches_oracle(pkg):
+    """glst_direct_coulomb (FP64 all pairs on the GPU) against the FP64 host
+    oracle; and GLST against it at 30,000 atoms, where the host direct sum is
+    slow: the GLST error vs the direct sum is the cubature's (~tol)."""
+    x, y, z, q = _water(700, 28.0, 12)
+    d = [_dev(a) for a in (x, y, z, q)]
+    outs = [torch.empty(len(x), dtype=torch.float64, device="cuda:0") for _ in range(4)]
+    pkg.direct_coulomb(*d, *outs)
+    torch.cuda.synchronize()
+    got = [o.cpu().numpy() for o in outs]
+    ref = oracle.coulomb(x, y, z, q)
+    rep = oracle.error_report(got, ref)
+    assert rep["force_rms_rel"] < 1e-13 and rep["energy_rel"] < 1e-13, rep
+
+
+@pytest.mark.parametrize("nshards", [2, 3, 5])
+def test_node_shards_sum_to_the_full_result(pkg, nshards):
+    """Multi-GPU node split on one device: the outputs of shards 0..n-1 add up
+    to the unsharded result (the reduction a multi-GPU caller does with NCCL)."""
+    n_mol, L, rcut, tol, seed = SYSTEMS["w2000_tol1e-5"]
+    x, y, z, q = _water(n_mol, L, seed)
+    d = [_dev(a) for a in (x, y, z, q)]
+    f, full = _run(pkg, x, y, z, q, tol, L, rcut)
+    e_full = f.energy()
+    f.close()
+    acc = [np.zeros(len(x)) for _ in range(4)]
+    e_sum = 0.0
+    for s in range(nshards):
+        with pkg.GlstForce(len(x), tol, L, L, L, rcut=rcut, shard=(s, nshards)) as g:
+            g.calc_ener_force(*d)
+            part = g.get_ef()
+            e_sum += g.energy()
+        for a, b in zip(acc, part):
+            a += b
+    rep = oracle.error_report(acc, full)
+    assert rep["force_rms_rel"] < 1e-12 and rep["energy_rel"] < 1e-12, rep
+    assert abs(e_sum - e_full) <= 1e-12 * abs(e_full)
+
+
+def test_autotune_keeps_results(pkg, store):
+    """glst_autotune changes launch shapes only: the tuned handle, and a new
+    handle of the same shape that inherits the tuning, stay within the parity
+    bars of the oracle."""
+    n_mol, L, rcut, tol, seed = SYSTEMS["w1000_c1tol"]
+    x, y, z, q = _water(n_mol, L, seed)
+    d = [_dev(a) for a in (x, y, z, q)]
+    p, ref = _oracle("w1000_c1tol", x, y, z, q, tol, L, rcut, store)
+    with pkg.GlstForce(len(x), tol, L, L, L, rcut=rcut) as f:
+        nb, waves = f.autotune(*d)
+        assert nb >= 1 and waves >= 2
+        f.calc_ener_force(*d)
+        got = f.get_ef()
+    rep = oracle.error_report(got, ref)
+    assert rep["force_rms_rel"] <= FORCE_RMS_TOL and rep["energy_rel"] <= ENERGY_TOL, rep
+    with pkg.GlstForce(len(x), tol, L, L, L, rcut=rcut) as f2:
+        f2.calc_ener_force(*d)
+        got2 = f2.get_ef()
+    rep2 = oracle.error_report(got2, ref)
+    assert rep2["force_rms_rel"] <= FORCE_RMS_TOL and rep2["energy_rel"] <= ENERGY_TOL, rep2

@@ -121,3 +121,19 @@ def test_reference_layout_directory_gives_same_plan(pkg, store, tmp_path):
     s2 = planner.TDesignStore(str(d))
     p = planner.make_plan(648, 1.676e-6, (18.63,) * 3, 9.0, s2)
     assert np.array_equal(p.kx, a[0])
+
+
+def test_charmm_roundtrip(tmp_path):
+    """psf/cor writer and reader use the columns the reference driver reads
+    (utils/io.cpp:35-117)."""
+    from glst_b200 import systems
+    x, y, z, q = systems.water_box(50, 12.0, seed=2)
+    systems.write_charmm(str(tmp_path / "w"), x, y, z, q)
+    a = systems.read_charmm(str(tmp_path / "w"))
+    for u, v in zip(a, (x, y, z, q)):
+        assert np.allclose(u, v, atol=1e-9, rtol=0)
+    lines = open(str(tmp_path / "w.psf")).read().splitlines()
+    hdr = [ln for ln in lines if "!NATOM" in ln][0]
+    assert hdr[11:17] == "!NATOM" and int(hdr[0:10]) == 150
+    r = systems.recenter(x + 3.0, y - 2.0, z)
+    assert min(a.min() for a in r) == 0.0
