@@ -1141,6 +1141,7 @@ glst_status glst_batch_system(glst_batch *b, uint32_t i, glst_handle **h) {
 //              requests that need a new system, off the launch path, so the
 //              GPU keeps working while new systems are set up.
 // A request's life: queued -> building (new system) -> ready -> running -> done.
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -1178,11 +1179,14 @@ struct SrvRequest {
 };
 
 struct SrvSlot {
-  cudaStream_t st = nullptr;
-  cudaEvent_t ev = nullptr;
+  cudaStream_t st_hi = nullptr, st_lo = nullptr;  // high priority for small requests
+  cudaStream_t st = nullptr;                      // the one in use
   double *pin = nullptr;  // 4N inputs, then 4N outputs + energy
   size_t cap = 0;         // atoms the pinned buffer holds
   SrvRequest *req = nullptr;
+  std::atomic<bool> gpu_done{false};  // set by the stream callback
+  SrvClock::time_point t_gpu_done;     // written before gpu_done
+  struct glst_server *owner = nullptr;
 };
 
 // Device bytes a handle for `p` will hold (an upper bound of setup's sizes).
@@ -1209,7 +1213,7 @@ struct glst_server {
   std::unordered_map<uint64_t, SrvRequest *> reqs;
   std::unordered_map<uint64_t, SrvSystem *> resident;  // named systems
   std::unordered_map<uint64_t, bool> building_key;      // keys with a system under construction
-  std::vector<SrvSlot> slots;
+  std::deque<SrvSlot> slots;  // stable addresses (stream callbacks point into it)
   std::vector<double *> old_pinned;    // outgrown staging, freed at destroy
   std::thread worker, builder;
   bool stop = false;          // worker: finish what is queued, then exit
@@ -1344,8 +1348,24 @@ static void srv_builder(glst_server *s) {
   }
 }
 
+// Stream callback at the end of a request's work: no CUDA calls here, only
+// the completion flag and a wake-up of the worker.
+// It must not take the server's lock: the worker holds it across CUDA calls
+// that may wait for pending callbacks (cudaFree synchronises the device).
+static void CUDART_CB srv_done_cb(void *arg) {
+  SrvSlot *sl = static_cast<SrvSlot *>(arg);
+  sl->t_gpu_done = SrvClock::now();
+  sl->gpu_done.store(true, std::memory_order_release);
+  sl->owner->cv_work.notify_all();
+}
+
+// Requests below this many atoms run on high-priority streams, so short
+// solves are not stuck behind the thread blocks of long ones.
+static constexpr uint32_t kSrvSmallAtoms = 20000;
+
 // Launch a ready request on a free slot (lock held).
 static void srv_launch(glst_server *s, SrvRequest *r, SrvSlot &sl) {
+  sl.st = r->natom < kSrvSmallAtoms ? sl.st_hi : sl.st_lo;
   SrvSystem *sys = r->sys;
   const size_t N = r->natom;
   if (sl.cap < N || !sl.pin) {
@@ -1378,7 +1398,10 @@ static void srv_launch(glst_server *s, SrvRequest *r, SrvSlot &sl) {
   if (st == GLST_OK &&
       cudaMemcpyAsync(sl.pin + 8 * N, h->energy, sizeof(double), cudaMemcpyDeviceToHost, sl.st) != cudaSuccess)
     st = fail(GLST_ERR_CUDA, "request energy copy failed");
-  if (st == GLST_OK && cudaEventRecord(sl.ev, sl.st) != cudaSuccess) st = fail(GLST_ERR_CUDA, "event record failed");
+  sl.gpu_done.store(false, std::memory_order_relaxed);
+  sl.owner = s;
+  if (st == GLST_OK && cudaLaunchHostFunc(sl.st, srv_done_cb, &sl) != cudaSuccess)
+    st = fail(GLST_ERR_CUDA, "completion callback failed");
   if (st != GLST_OK) {
     cudaStreamSynchronize(sl.st);
     sys->busy = false;
@@ -1396,11 +1419,11 @@ static void srv_worker(glst_server *s) {
   std::unique_lock<std::mutex> lk(s->mu);
   while (true) {
     bool progress = false;
-    // 1. complete requests whose work finished
+    // 1. complete requests whose work finished (flag set by the callback)
     for (auto &sl : s->slots) {
-      if (!sl.req) continue;
-      const cudaError_t q = cudaEventQuery(sl.ev);
-      if (q == cudaErrorNotReady) continue;
+      if (!sl.req || !sl.gpu_done.load(std::memory_order_acquire)) continue;
+      cudaError_t q = cudaStreamQuery(sl.st);
+      if (q == cudaErrorNotReady) q = cudaSuccess;  // only the callback itself is still returning
       SrvRequest *r = sl.req;
       const size_t N = r->natom;
       if (q == cudaSuccess) {
@@ -1414,6 +1437,8 @@ static void srv_worker(glst_server *s) {
       s->stats.in_flight--;
       srv_finish(s, r, q == cudaSuccess ? GLST_OK : GLST_ERR_CUDA,
                  q == cudaSuccess ? nullptr : cudaGetErrorString(q));
+      r->t_done = sl.t_gpu_done;  // completion time as the GPU finished it
+      sl.gpu_done.store(false, std::memory_order_relaxed);
       progress = true;
     }
     // 2. admit queued requests (they keep their place if they cannot start:
@@ -1442,13 +1467,15 @@ static void srv_worker(glst_server *s) {
       ++it;
     }
     if (s->stop && s->queue.empty() && s->stats.in_flight == 0) break;
-    // Sleep, releasing the lock: briefly while GPU work is in flight (its
-    // completion is polled), otherwise until a submit or a finished build
-    // notifies -- unless this pass made progress, which may unblock more.
-    if (s->stats.in_flight)
-      s->cv_work.wait_for(lk, std::chrono::microseconds(20));
-    else if (!progress)
-      s->cv_work.wait_for(lk, std::chrono::milliseconds(5));
+    // Sleep, releasing the lock, until a submit, a finished build or a
+    // completion callback notifies -- unless this pass made progress, which
+    // may unblock more.  The timeout is only a safety net.
+    if (!progress) {
+      bool any_done = false;
+      for (auto &sl : s->slots) any_done |= (sl.req && sl.gpu_done.load(std::memory_order_acquire));
+      // short timeout: a callback's notify can land just before this wait
+      if (!any_done) s->cv_work.wait_for(lk, std::chrono::microseconds(s->stats.in_flight ? 100 : 5000));
+    }
   }
 }
 
@@ -1461,10 +1488,13 @@ glst_status glst_server_create(glst_server **out, uint64_t budget_bytes, uint32_
   CUDA_TRY(cudaGetDevice(&s->device));
   CUDA_TRY(cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, s->device));
   s->budget = budget_bytes;
-  s->slots.resize(std::max<uint32_t>(1, nslots));
+  for (uint32_t i = 0; i < std::max<uint32_t>(1, nslots); i++) s->slots.emplace_back();
+  int prio_lo = 0, prio_hi = 0;
+  CUDA_TRY(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
   for (auto &sl : s->slots) {
-    CUDA_TRY(cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking));
-    CUDA_TRY(cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming));
+    CUDA_TRY(cudaStreamCreateWithPriority(&sl.st_hi, cudaStreamNonBlocking, prio_hi));
+    CUDA_TRY(cudaStreamCreateWithPriority(&sl.st_lo, cudaStreamNonBlocking, prio_lo));
+    sl.st = sl.st_lo;
   }
   glst_server *raw = s.release();
   raw->worker = std::thread(srv_worker, raw);
@@ -1494,8 +1524,8 @@ glst_status glst_server_destroy(glst_server *s) {
   for (auto *sys : left) srv_drop_system(s, sys);
   for (auto &sl : s->slots) {
     if (sl.pin) cudaFreeHost(sl.pin);
-    cudaStreamDestroy(sl.st);
-    cudaEventDestroy(sl.ev);
+    cudaStreamDestroy(sl.st_hi);
+    cudaStreamDestroy(sl.st_lo);
   }
   for (double *p : s->old_pinned) cudaFreeHost(p);
   for (auto &kv : s->reqs) delete kv.second;

@@ -26,6 +26,14 @@ struct Grid {
   int ct_float;   // bin in float arithmetic (glst_force<float>)
 };
 
+// SFU sine and cosine of an FP32 angle in radians (PTX sin/cos.approx,
+// flush-to-zero).  Absolute error ~1e-6 for the |x| < ~30 rad used here,
+// below the FP32 rounding of the phase itself at that magnitude.
+__device__ __forceinline__ void sfu_sincos(float x, float *s, float *c) {
+  asm("sin.approx.ftz.f32 %0, %1;" : "=f"(*s) : "f"(x));
+  asm("cos.approx.ftz.f32 %0, %1;" : "=f"(*c) : "f"(x));
+}
+
 __device__ __forceinline__ double cell_centre(uint32_t i, double l) {
   return (static_cast<double>(i) + 0.5) * l;
 }
@@ -228,7 +236,7 @@ k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ 
         for (int u = 0; u < kSfNodesPerThread; u++) {
           const float th = fmaf(kx[u], p.x, fmaf(ky[u], p.y, kz[u] * p.z));
           float s, c;
-          __sincosf(th, &s, &c);
+          sfu_sincos(th, &s, &c);
           fr[u] = fmaf(p.w, c, fr[u]);
           fi[u] = fmaf(-p.w, s, fi[u]);
         }
@@ -319,6 +327,7 @@ k_shell_sums(Grid g, SatArgs a) {
     s_tw[t] = make_double2(cs, sn);
   }
   // load S[c][k0 .. k0+nb) -> s_sat[j*stride + c]
+#pragma unroll 4
   for (uint32_t t = threadIdx.x; t < C * nb; t += blockDim.x) {
     const uint32_t c = t / nb, j = t % nb;
     s_sat[j * a.stride + c] = a.S[(size_t)c * a.K + k0 + j];
@@ -404,7 +413,7 @@ __device__ __forceinline__ void lr_prefetch(float2 (&pre)[kLrPerThread], const f
   }
 }
 
-__global__ void __launch_bounds__(kLrThreads, 12)
+__global__ void __launch_bounds__(kLrThreads, 10)
 k_long_range(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_count,
              const uint32_t *__restrict__ cell_point, const LrChunk *__restrict__ chunks,
              const float4 *__restrict__ dirs, const float *__restrict__ kappa,
@@ -449,17 +458,34 @@ k_long_range(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_co
         for (uint32_t d = 0; d < nd; d++) {
           const float4 sj = dirs[ch.dir_begin + d0 + d];
           const float u = fmaf(sj.x, p.x, fmaf(sj.y, p.y, sj.z * p.z));
-          float e = 0.f, gsum = 0.f;
+          // Two accumulator sets (even / odd r) and split energy terms keep
+          // the FMA dependency chains short, so a warp is not limited by
+          // accumulator latency before the SFU pipe is full.
+          float ea = 0.f, eb = 0.f, ec = 0.f, ed = 0.f, ga = 0.f, gb = 0.f;
           const float4 *nn = buf + d * nr;
-#pragma unroll 4
-          for (uint32_t r = 0; r < nr; r++) {
-            const float4 v = nn[r];
-            float sn, cs;
-            __sincosf(v.z * u, &sn, &cs);
-            e = fmaf(cs, v.x, e);
-            e = fmaf(-sn, v.y, e);
-            gsum = fmaf(v.z, fmaf(cs, v.y, sn * v.x), gsum);
+          uint32_t r = 0;
+#pragma unroll 2
+          for (; r + 1 < nr; r += 2) {
+            const float4 v0 = nn[r], v1 = nn[r + 1];
+            float s0, c0, s1, c1;
+            sfu_sincos(v0.z * u, &s0, &c0);
+            sfu_sincos(v1.z * u, &s1, &c1);
+            ea = fmaf(c0, v0.x, ea);
+            eb = fmaf(-s0, v0.y, eb);
+            ec = fmaf(c1, v1.x, ec);
+            ed = fmaf(-s1, v1.y, ed);
+            ga = fmaf(v0.z, fmaf(c0, v0.y, s0 * v0.x), ga);
+            gb = fmaf(v1.z, fmaf(c1, v1.y, s1 * v1.x), gb);
           }
+          if (r < nr) {
+            const float4 v0 = nn[r];
+            float s0, c0;
+            sfu_sincos(v0.z * u, &s0, &c0);
+            ea = fmaf(c0, v0.x, ea);
+            eb = fmaf(-s0, v0.y, eb);
+            ga = fmaf(v0.z, fmaf(c0, v0.y, s0 * v0.x), ga);
+          }
+          const float e = (ea + eb) + (ec + ed), gsum = ga + gb;
           te += e;
           tx = fmaf(gsum, sj.x, tx);
           ty = fmaf(gsum, sj.y, ty);
@@ -653,7 +679,7 @@ __global__ void k_probe_sfu(float *out, int iters) {
 #pragma unroll
     for (int u = 0; u < 8; u++) {
       float s, c;
-      __sincosf(a[u], &s, &c);
+      sfu_sincos(a[u], &s, &c);
       a[u] = s + c;  // 2 MUFU + 1 FADD
     }
   }

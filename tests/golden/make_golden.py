@@ -41,9 +41,11 @@ CASES = {
     # one million atoms; stored as a seeded subset of atoms plus
     # digests of the full assignment (the full arrays would be 36 MB)
     "water333k": (333333, 215.3, 10.0, math.erfc(0.31 * 10.0) / 10.0, 0),
+    # configs[1] at the next higher cubature order (tol / 10)
+    "water10k_next": (10000, 66.9, 10.0, math.erfc(0.31 * 10.0) / 100.0, 0),
 }
 SUBSET = {"water333k": 20000}
-CASE_CTS = {"water333k": ("double",)}
+CASE_CTS = {"water333k": ("double",), "water10k_next": ("double",)}
 CTS = ("double", "float")
 
 

@@ -40,6 +40,7 @@ def test_fixtures_present():
         for ct in ("double", "float"):
             assert "%s_%s.npz" % (c, ct) in names
     assert "water333k_double.npz" in names
+    assert "water10k_next_double.npz" in names
 
 
 @pytest.mark.parametrize("case", SMALL)

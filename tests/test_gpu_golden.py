@@ -66,3 +66,20 @@ def test_water333k_matches_reference_subset(pkg):
     print("water333k force_rms_rel(subset) %.3e energy_rel %.3e" % (rel, e_rel))
     assert rel <= FORCE_RMS_TOL
     assert e_rel <= ENERGY_TOL
+
+
+def test_water10k_next_order_matches_reference(pkg):
+    """configs[1] at the next higher cubature order (tol/10: t = 101, 83, 57,
+    K = 192,478 nodes) against the reference's glst_force<double>."""
+    d, (x, y, z, q), box = load_case("water10k_next", "double")
+    dev = [torch.tensor(a, dtype=torch.float64, device="cuda:0") for a in (x, y, z, q)]
+    with pkg.GlstForce(len(x), float(d["tol"]), *box, rcut=float(d["rcut"])) as f:
+        assert f.info().num_nodes == int(d["K"])
+        f.calc_ener_force(*dev)
+        got = f.get_ef()
+        sidx, cnt, pnt = f.assignment()
+    assert np.array_equal(sidx, d["sorted_idx"])
+    rep = oracle.error_report(got, (d["fx"], d["fy"], d["fz"], d["en"]))
+    print("water10k_next", rep)
+    assert rep["force_rms_rel"] <= FORCE_RMS_TOL, rep
+    assert rep["energy_rel"] <= ENERGY_TOL, rep
