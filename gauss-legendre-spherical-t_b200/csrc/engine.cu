@@ -125,6 +125,11 @@ struct glst_handle {
   uint32_t combine_blocks = 1;
   bool computed = false;
   std::vector<DevBuf> bufs;
+  struct PendingBuf {
+    void **out;
+    size_t bytes;
+  };
+  std::vector<PendingBuf> pending;  // requested, not yet carved (setup)
   uint64_t bytes = 0;
   // atoms
   uint32_t *atom_cell = nullptr, *atom_slot = nullptr, *perm = nullptr;
@@ -155,17 +160,35 @@ struct glst_handle {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
+// Buffers of a handle are requested first and then carved out of one
+// allocation (commit_allocs): one cudaMalloc per system keeps set-up cheap
+// for servers that create systems while others compute.
 static glst_status dalloc(glst_handle *h, void **out, size_t bytes) {
   *out = nullptr;
-  if (bytes == 0) bytes = 16;
-  cudaError_t e = cudaMalloc(out, bytes);
+  h->pending.push_back({out, std::max<size_t>(bytes, 16)});
+  return GLST_OK;
+}
+
+static glst_status commit_allocs(glst_handle *h) {
+  auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+  size_t total = 0;
+  for (const auto &p : h->pending) total += al(p.bytes);
+  if (!total) return GLST_OK;
+  void *base = nullptr;
+  const cudaError_t e = cudaMalloc(&base, total);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    return fail(GLST_ERR_OUT_OF_MEMORY, "cudaMalloc(%zu bytes) failed: %s", bytes,
-                cudaGetErrorString(e));
+    h->pending.clear();
+    return fail(GLST_ERR_OUT_OF_MEMORY, "cudaMalloc(%zu bytes) failed: %s", total, cudaGetErrorString(e));
   }
-  h->bufs.push_back({*out, bytes});
-  h->bytes += bytes;
+  h->bufs.push_back({base, total});
+  h->bytes += total;
+  size_t off = 0;
+  for (const auto &p : h->pending) {
+    *p.out = static_cast<char *>(base) + off;
+    off += al(p.bytes);
+  }
+  h->pending.clear();
   return GLST_OK;
 }
 
@@ -177,6 +200,7 @@ static glst_status dalloc_n(glst_handle *h, T **out, size_t n) {
 static void release(glst_handle *h) {
   for (auto &b : h->bufs) cudaFree(b.p);
   h->bufs.clear();
+  h->pending.clear();
   if (h->chunks) cudaFree(h->chunks);
   if (h->part) cudaFree(h->part);
   h->chunks = nullptr;
@@ -311,12 +335,12 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
   // Nodes and weights are rounded to CT first, as the reference stores them
   // (src/cubature.cu:138-141).
   std::vector<uint32_t> kappa_base, dir_base, node_base;
+  std::vector<float4> n32(K);
+  std::vector<double4> n64(K);
+  std::vector<uint32_t> radii(K);
+  std::vector<float4> dirs;
+  std::vector<float> kap;
   {
-    std::vector<float4> n32(K);
-    std::vector<double4> n64(K);
-    std::vector<uint32_t> radii(K);
-    std::vector<float4> dirs;
-    std::vector<float> kap;
     uint32_t ref_base = 0, ibase = 0;
     for (size_t gi = 0; gi < (K ? p.groups.size() : 0); gi++) {
       const auto &g = p.groups[gi];
@@ -349,13 +373,6 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
     GLST_TRY(dalloc_n(h, &h->node_radii, K));
     GLST_TRY(dalloc_n(h, &h->dirs, dirs.size()));
     GLST_TRY(dalloc_n(h, &h->kappa, kap.size()));
-    if (K) {
-      CUDA_TRY(cudaMemcpy(h->node32, n32.data(), K * sizeof(float4), cudaMemcpyHostToDevice));
-      CUDA_TRY(cudaMemcpy(h->node64, n64.data(), K * sizeof(double4), cudaMemcpyHostToDevice));
-      CUDA_TRY(cudaMemcpy(h->node_radii, radii.data(), K * sizeof(uint32_t), cudaMemcpyHostToDevice));
-      CUDA_TRY(cudaMemcpy(h->dirs, dirs.data(), dirs.size() * sizeof(float4), cudaMemcpyHostToDevice));
-      CUDA_TRY(cudaMemcpy(h->kappa, kap.data(), kap.size() * sizeof(float), cudaMemcpyHostToDevice));
-    }
   }
   GLST_TRY(dalloc_n(h, &h->atom_cell, N));
   GLST_TRY(dalloc_n(h, &h->atom_slot, N));
@@ -414,6 +431,14 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
     GLST_TRY(build_chunks(h));
     GLST_TRY(dalloc_n(h, &h->S, C * (size_t)h->K));
     GLST_TRY(dalloc_n(h, &h->R, C * (size_t)h->K));
+  }
+  GLST_TRY(commit_allocs(h));
+  if (K) {
+    CUDA_TRY(cudaMemcpy(h->node32, n32.data(), K * sizeof(float4), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->node64, n64.data(), K * sizeof(double4), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->node_radii, radii.data(), K * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->dirs, dirs.data(), dirs.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->kappa, kap.data(), kap.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
   if (shard > 0) CUDA_TRY(cudaMemset(h->sr, 0, (size_t)dev::kSrPlanes * N * sizeof(double4)));
   CUDA_TRY(cudaFuncSetAttribute(dev::k_sort_pack, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -937,6 +962,8 @@ struct glst_batch {
   double *energies = nullptr;           // device, one per system
 };
 
+static constexpr uint32_t kBatchLargeAtoms = 20000;  // fills the GPU by itself
+
 static void batch_release(glst_batch *b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
@@ -1050,14 +1077,19 @@ glst_status glst_batch_create(glst_batch **out, uint32_t nsys, const uint32_t *n
     b->branch.push_back(st);
     b->branch_done.push_back(ev);
   }
-  // largest first onto the least loaded branch
+  // Systems large enough to fill the GPU alone run one after another on
+  // branch 0 (running two at once only splits the SMs between them); the
+  // rest go largest first onto the least loaded of the other branches, where
+  // they fill the SMs the large ones leave idle.
   b->order.resize(nsys);
   for (uint32_t i = 0; i < nsys; i++) b->order[i] = i;
   std::stable_sort(b->order.begin(), b->order.end(), [&](uint32_t a, uint32_t c) { return cost[a] > cost[c]; });
   std::vector<double> load(ns, 0.0);
   b->branch_of.assign(nsys, 0);
   for (uint32_t i : b->order) {
-    const uint32_t j = (uint32_t)(std::min_element(load.begin(), load.end()) - load.begin());
+    uint32_t j = 0;
+    if (ns > 1 && natom[i] < kBatchLargeAtoms)
+      j = 1 + (uint32_t)(std::min_element(load.begin() + 1, load.end()) - (load.begin() + 1));
     b->branch_of[i] = j;
     load[j] += cost[i];
   }
@@ -1179,8 +1211,7 @@ struct SrvRequest {
 };
 
 struct SrvSlot {
-  cudaStream_t st_hi = nullptr, st_lo = nullptr;  // high priority for small requests
-  cudaStream_t st = nullptr;                      // the one in use
+  cudaStream_t st = nullptr;
   double *pin = nullptr;  // 4N inputs, then 4N outputs + energy
   size_t cap = 0;         // atoms the pinned buffer holds
   SrvRequest *req = nullptr;
@@ -1220,6 +1251,7 @@ struct glst_server {
   bool stop_builder = false;  // builder: exit (set after the worker has finished)
   uint64_t next_ticket = 1, clock = 0;
   uint64_t reserved = 0;               // bytes promised to systems being built
+  uint32_t large_in_flight = 0;        // running requests of >= kSrvSmallAtoms atoms
   glst_server_stats stats{};
 };
 
@@ -1359,13 +1391,13 @@ static void CUDART_CB srv_done_cb(void *arg) {
   sl->owner->cv_work.notify_all();
 }
 
-// Requests below this many atoms run on high-priority streams, so short
-// solves are not stuck behind the thread blocks of long ones.
+// Requests of at least this many atoms fill the GPU by themselves.
 static constexpr uint32_t kSrvSmallAtoms = 20000;
 
-// Launch a ready request on a free slot (lock held).
+// Launch a ready request on a free slot (lock held).  All slots have equal
+// stream priority: giving small requests priority starved the large ones
+// under overload (their thread blocks kept losing the SMs).
 static void srv_launch(glst_server *s, SrvRequest *r, SrvSlot &sl) {
-  sl.st = r->natom < kSrvSmallAtoms ? sl.st_hi : sl.st_lo;
   SrvSystem *sys = r->sys;
   const size_t N = r->natom;
   if (sl.cap < N || !sl.pin) {
@@ -1426,6 +1458,7 @@ static void srv_worker(glst_server *s) {
       if (q == cudaErrorNotReady) q = cudaSuccess;  // only the callback itself is still returning
       SrvRequest *r = sl.req;
       const size_t N = r->natom;
+      if (r->natom >= kSrvSmallAtoms) s->large_in_flight--;
       if (q == cudaSuccess) {
         r->out.assign(sl.pin + 4 * N, sl.pin + 8 * N);
         r->energy = sl.pin[8 * N];
@@ -1450,7 +1483,10 @@ static void srv_worker(glst_server *s) {
         it = s->queue.erase(it);
         continue;
       }
-      if (r->state == SrvState::Ready) {
+      // A large request fills the GPU by itself: run one at a time (two
+      // would only split the SMs between them); small ones fill the gaps.
+      const bool large = r->natom >= kSrvSmallAtoms;
+      if (r->state == SrvState::Ready && !(large && s->large_in_flight > 0)) {
         SrvSlot *free_slot = nullptr;
         for (auto &sl : s->slots)
           if (!sl.req) {
@@ -1459,6 +1495,7 @@ static void srv_worker(glst_server *s) {
           }
         if (free_slot) {
           srv_launch(s, r, *free_slot);
+          if (large && r->state == SrvState::Running) s->large_in_flight++;
           it = s->queue.erase(it);
           progress = true;
           continue;
@@ -1489,12 +1526,11 @@ glst_status glst_server_create(glst_server **out, uint64_t budget_bytes, uint32_
   CUDA_TRY(cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, s->device));
   s->budget = budget_bytes;
   for (uint32_t i = 0; i < std::max<uint32_t>(1, nslots); i++) s->slots.emplace_back();
-  int prio_lo = 0, prio_hi = 0;
-  CUDA_TRY(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
   for (auto &sl : s->slots) {
-    CUDA_TRY(cudaStreamCreateWithPriority(&sl.st_hi, cudaStreamNonBlocking, prio_hi));
-    CUDA_TRY(cudaStreamCreateWithPriority(&sl.st_lo, cudaStreamNonBlocking, prio_lo));
-    sl.st = sl.st_lo;
+    CUDA_TRY(cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking));
+    // staging for requests up to 262,144 atoms; larger ones grow it
+    sl.cap = 262144;
+    CUDA_TRY(cudaHostAlloc(reinterpret_cast<void **>(&sl.pin), (8 * sl.cap + 1) * sizeof(double), 0));
   }
   glst_server *raw = s.release();
   raw->worker = std::thread(srv_worker, raw);
@@ -1524,8 +1560,7 @@ glst_status glst_server_destroy(glst_server *s) {
   for (auto *sys : left) srv_drop_system(s, sys);
   for (auto &sl : s->slots) {
     if (sl.pin) cudaFreeHost(sl.pin);
-    cudaStreamDestroy(sl.st_hi);
-    cudaStreamDestroy(sl.st_lo);
+    cudaStreamDestroy(sl.st);
   }
   for (double *p : s->old_pinned) cudaFreeHost(p);
   for (auto &kv : s->reqs) delete kv.second;

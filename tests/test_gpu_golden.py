@@ -34,11 +34,13 @@ def test_cuda_path_matches_reference(pkg, case, ct):
     assert np.array_equal(sidx, d["sorted_idx"])
     assert np.array_equal(cnt, d["cell_count"])
     assert np.array_equal(pnt, d["cell_point"])
-    if ct == "double":
-        rep = oracle.error_report(got, (d["fx"], d["fy"], d["fz"], d["en"]))
-        print(case, ct, rep)
-        assert rep["force_rms_rel"] <= FORCE_RMS_TOL, rep
-        assert rep["energy_rel"] <= ENERGY_TOL, rep
+    # against the reference of the same CT: glst_force<double> is FP64
+    # throughout; glst_force<float> carries its own ~1e-6 float error, which
+    # the same bars still cover
+    rep = oracle.error_report(got, (d["fx"], d["fy"], d["fz"], d["en"]))
+    print(case, ct, rep)
+    assert rep["force_rms_rel"] <= FORCE_RMS_TOL, rep
+    assert rep["energy_rel"] <= ENERGY_TOL, rep
 
 
 def test_water333k_matches_reference_subset(pkg):

@@ -331,3 +331,20 @@ def test_autotune_keeps_results(pkg, store):
         got2 = f2.get_ef()
     rep2 = oracle.error_report(got2, ref)
     assert rep2["force_rms_rel"] <= FORCE_RMS_TOL and rep2["energy_rel"] <= ENERGY_TOL, rep2
+
+
+def test_init_and_ncell_constructor(pkg, store):
+    """glst_force::init re-plans an existing object (src/glst_force.cu:179-327);
+    the ncell constructor uses rcut = min(L/n) (src/glst_force.cu:80-95)."""
+    n_mol, L, rcut, tol, seed = SYSTEMS["w1000_tol1e-4"]
+    x, y, z, q = _water(n_mol, L, seed)
+    with pkg.GlstForce(300, 1e-5, 20.0, 20.0, 20.0, rcut=10.0) as f:
+        f.init(len(x), tol, L, L, L, rcut)
+        f.calc_ener_force(*[_dev(a) for a in (x, y, z, q)])
+        got = f.get_ef()
+    p, ref = _oracle("w1000_tol1e-4", x, y, z, q, tol, L, rcut, store)
+    rep = oracle.error_report(got, ref)
+    assert rep["force_rms_rel"] <= FORCE_RMS_TOL and rep["energy_rel"] <= ENERGY_TOL, rep
+    with pkg.GlstForce(len(x), tol, L, L, L, ncell=(4, 4, 4)) as g:
+        assert tuple(g.info().ncell) == (4, 4, 4)
+        assert g.info().cell_dim == L / 4
