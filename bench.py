@@ -138,6 +138,7 @@ def cpu_baseline_run(sysd, K_sample_div=32):
 
 
 def run_reference(args, world, rank):
+    __graft_entry__.load_package()
     from glst_b200 import systems
     if rank != 0:
         return
@@ -378,7 +379,7 @@ def run_ours(args, world, rank, local, dist):
         "clocks": clk,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 4 * 8 * n, "d2h_bytes_per_step": 4 * 8 * n,
                 "path": "glst_compute_host (pinned host buffers, H2D + solve + D2H per step)"},
-        "gpu_launches": 10 * args.steps,
+        "gpu_launches": int(inf.kernels_per_compute) * args.steps,
         "phases_ms": phases,
         "roofline": roofline,
         "wall_s_timed": wall,

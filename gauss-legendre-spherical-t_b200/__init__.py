@@ -50,6 +50,7 @@ class GlstInfo(ctypes.Structure):
         ("group_r_in", ctypes.c_uint32 * 16),
         ("group_r_out", ctypes.c_uint32 * 16),
         ("device_bytes", ctypes.c_uint64),
+        ("kernels_per_compute", ctypes.c_uint32),
     ]
 
 

@@ -155,9 +155,13 @@ struct glst_handle {
   double *block_energy = nullptr, *energy = nullptr;
   // host-visible staging for the end-to-end path
   double *in_host = nullptr;  // device copy of host inputs (4 x natom)
-  // streams/events for the near-field fork
-  cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // streams/events for the near-field fork and the far-field pipeline
+  cudaStream_t side = nullptr, far2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_far2 = nullptr;
+  struct FarRange {
+    uint32_t kb, ke, c0, c1;  // nodes and long-range chunks of one pipeline stage
+  };
+  std::vector<FarRange> ranges;
 };
 
 // Buffers of a handle are requested first and then carved out of one
@@ -208,10 +212,12 @@ static void release(glst_handle *h) {
   h->part_cap = 0;
   h->bytes = 0;
   if (h->side) cudaStreamDestroy(h->side);
+  if (h->far2) cudaStreamDestroy(h->far2);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
   if (h->ev_join) cudaEventDestroy(h->ev_join);
-  h->side = nullptr;
-  h->ev_fork = h->ev_join = nullptr;
+  if (h->ev_far2) cudaEventDestroy(h->ev_far2);
+  h->side = h->far2 = nullptr;
+  h->ev_fork = h->ev_join = h->ev_far2 = nullptr;
 }
 
 // ---------------------------------------------------------------- tuning
@@ -234,6 +240,8 @@ static Tuning tuned(const Plan &p, uint32_t K) {
   auto it = g_tune.find(tune_key(p, K));
   return it == g_tune.end() ? Tuning{} : it->second;
 }
+
+static constexpr uint32_t kFarStages = 1;  // far-field pipeline stages per solve (see below)
 
 // Long-range chunks: whole directions of one group each, sized so that
 // ncell x chunks is about lr_waves waves of resident CTAs; then this
@@ -279,6 +287,22 @@ static glst_status build_chunks(glst_handle *h) {
   }
   if (chunks.size() > 65535) return fail(GLST_ERR_SIZE, "too many long-range chunks");
   h->nsplit = (uint32_t)chunks.size();
+  // pipeline stages: about kFarStages chunk-aligned node ranges
+  h->ranges.clear();
+  {
+    const uint32_t stages = std::min<uint32_t>(kFarStages, h->nsplit);
+    uint32_t c0 = 0;
+    for (uint32_t s = 0; s < stages && c0 < h->nsplit; s++) {
+      const uint64_t target = (uint64_t)h->K * (s + 1) / stages;  // local node count at the stage end
+      uint32_t c1 = c0 + 1;
+      while (c1 < h->nsplit && chunks[c1].node_begin < target) c1++;
+      if (s + 1 == stages) c1 = h->nsplit;
+      const uint32_t kb = chunks[c0].node_begin;
+      const uint32_t ke = chunks[c1 - 1].node_begin + chunks[c1 - 1].n_dir * chunks[c1 - 1].n_rad;
+      h->ranges.push_back({kb, ke, c0, c1});
+      c0 = c1;
+    }
+  }
   if (h->chunks) {
     cudaFree(h->chunks);
     h->bytes -= h->chunk_bytes;
@@ -444,8 +468,10 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
   CUDA_TRY(cudaFuncSetAttribute(dev::k_sort_pack, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(dev::kSortCap * sizeof(uint32_t))));
   CUDA_TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+  CUDA_TRY(cudaStreamCreateWithFlags(&h->far2, cudaStreamNonBlocking));
   CUDA_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&h->ev_far2, cudaEventDisableTiming));
   CUDA_TRY(cudaMemset(h->flags, 0, 4 * sizeof(uint32_t)));
   h->computed = false;
   return GLST_OK;
@@ -478,35 +504,51 @@ static glst_status phase_assign(glst_handle *h, const double *rx, const double *
   return GLST_OK;
 }
 
-static glst_status phase_sf(glst_handle *h, cudaStream_t st) {
-  if (!h->K || !h->plan.natom) return GLST_OK;
+// Far-field phases over a range of the handle's nodes [kb, ke) (local,
+// internal order) and of its long-range chunks [c0, c1).
+static glst_status sf_range(glst_handle *h, uint32_t kb, uint32_t ke, cudaStream_t st) {
+  if (ke <= kb || !h->plan.natom) return GLST_OK;
   const uint32_t per = dev::kSfThreads * dev::kSfNodesPerThread;
   const uint32_t cg = (h->plan.ncell + dev::kSfCellsPerCta - 1) / dev::kSfCellsPerCta;
   if (cg > 65535) return fail(GLST_ERR_SIZE, "too many cells for the structure-factor grid");
-  dim3 grid((h->K + per - 1) / per, cg);
-  dev::k_structure_factors<<<grid, dev::kSfThreads, 0, st>>>(h->pk, h->cell_count, h->cell_point, h->grid,
-                                                             h->node32 + h->k_begin, h->node64 + h->k_begin,
-                                                             h->K, h->S);
+  dim3 grid((ke - kb + per - 1) / per, cg);
+  dev::k_structure_factors<<<grid, dev::kSfThreads, 0, st>>>(
+      h->pk, h->cell_count, h->cell_point, h->grid, h->node32 + h->k_begin + kb, h->node64 + h->k_begin + kb,
+      ke - kb, h->K, h->S + kb);
   CUDA_TRY(cudaGetLastError());
   return GLST_OK;
 }
 
-static glst_status phase_shell(glst_handle *h, cudaStream_t st) {
-  if (!h->K || !h->plan.natom) return GLST_OK;
-  dev::SatArgs a{h->S, h->node64 + h->k_begin, h->node_radii + h->k_begin, h->K, h->sat_nb, h->sat_stride, h->R};
-  const uint32_t nblk = (h->K + h->sat_nb - 1) / h->sat_nb;
+static glst_status shell_range(glst_handle *h, uint32_t kb, uint32_t ke, cudaStream_t st) {
+  if (ke <= kb || !h->plan.natom) return GLST_OK;
+  dev::SatArgs a{h->S + kb, h->node64 + h->k_begin + kb, h->node_radii + h->k_begin + kb, ke - kb, h->K,
+                 h->sat_nb, h->sat_stride, h->R + kb};
+  const uint32_t nblk = (ke - kb + h->sat_nb - 1) / h->sat_nb;
   dev::k_shell_sums<<<nblk, dev::kSatThreads, h->sat_smem, st>>>(h->grid, a);
   CUDA_TRY(cudaGetLastError());
   return GLST_OK;
 }
 
-static glst_status phase_lr(glst_handle *h, cudaStream_t st) {
-  if (!h->K || !h->plan.natom) return GLST_OK;
-  dim3 grid(h->plan.ncell, h->nsplit);
-  dev::k_long_range<<<grid, dev::kLrThreads, 0, st>>>(h->pk, h->cell_count, h->cell_point, h->chunks, h->dirs,
-                                                      h->kappa, h->R, h->K, h->plan.natom, h->part);
+static glst_status lr_range(glst_handle *h, uint32_t c0, uint32_t c1, cudaStream_t st) {
+  if (c1 <= c0 || !h->plan.natom) return GLST_OK;
+  dim3 grid(h->plan.ncell, c1 - c0);
+  dev::k_long_range<<<grid, dev::kLrThreads, 0, st>>>(h->pk, h->cell_count, h->cell_point, h->chunks + c0,
+                                                      h->dirs, h->kappa, h->R, h->K, h->plan.natom,
+                                                      h->part + (size_t)c0 * h->plan.natom);
   CUDA_TRY(cudaGetLastError());
   return GLST_OK;
+}
+
+static glst_status phase_sf(glst_handle *h, cudaStream_t st) {
+  return h->K ? sf_range(h, 0, h->K, st) : GLST_OK;
+}
+
+static glst_status phase_shell(glst_handle *h, cudaStream_t st) {
+  return h->K ? shell_range(h, 0, h->K, st) : GLST_OK;
+}
+
+static glst_status phase_lr(glst_handle *h, cudaStream_t st) {
+  return h->K ? lr_range(h, 0, h->nsplit, st) : GLST_OK;
 }
 
 static glst_status phase_sr(glst_handle *h, cudaStream_t st) {
@@ -543,9 +585,23 @@ static glst_status compute_all(glst_handle *h, const double *rx, const double *r
   CUDA_TRY(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
   GLST_TRY(phase_sr(h, h->side));
   CUDA_TRY(cudaEventRecord(h->ev_join, h->side));
-  GLST_TRY(phase_sf(h, st));
-  GLST_TRY(phase_shell(h, st));
-  GLST_TRY(phase_lr(h, st));
+  // Far field in node ranges, alternating between two streams so that the
+  // shell sums of one range (shared-memory bound) could overlap the SFU-bound
+  // kernels of the next.  Measured on B200 it does not: the structure-factor
+  // kernel fills every SM's register file, so the other stream's blocks only
+  // start as it drains.  kFarStages is therefore 1 (the plain sequence).
+  if (h->K && h->plan.natom && !h->ranges.empty()) {
+    CUDA_TRY(cudaStreamWaitEvent(h->far2, h->ev_fork, 0));
+    for (size_t r = 0; r < h->ranges.size(); r++) {
+      const auto &rg = h->ranges[r];
+      cudaStream_t s = (r & 1) ? h->far2 : st;
+      GLST_TRY(sf_range(h, rg.kb, rg.ke, s));
+      GLST_TRY(shell_range(h, rg.kb, rg.ke, s));
+      GLST_TRY(lr_range(h, rg.c0, rg.c1, s));
+    }
+    CUDA_TRY(cudaEventRecord(h->ev_far2, h->far2));
+    CUDA_TRY(cudaStreamWaitEvent(st, h->ev_far2, 0));
+  }
   CUDA_TRY(cudaStreamWaitEvent(st, h->ev_join, 0));
   return phase_combine(h, st);
 }
@@ -785,6 +841,9 @@ glst_status glst_get_info(const glst_handle *h, glst_info *info) {
   DeviceGuard guard_(h);
   fill_info(h->plan, info);
   info->device_bytes = h->bytes;
+  // assignment 4 (+0 without atoms), near field 1, far field 3 per stage, combine 2
+  info->kernels_per_compute =
+      h->plan.natom ? 4u + (h->shard == 0 ? 1u : 0u) + 3u * (uint32_t)(h->K ? h->ranges.size() : 0) + 2u : 2u;
   return GLST_OK;
 }
 

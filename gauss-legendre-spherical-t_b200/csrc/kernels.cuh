@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(kSfThreads)
 k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_count,
                     const uint32_t *__restrict__ cell_point, Grid g,
                     const float4 *__restrict__ node32, const double4 *__restrict__ node64,
-                    uint32_t K, double2 *__restrict__ S) {
+                    uint32_t K, uint32_t ld, double2 *__restrict__ S) {
   __shared__ float4 s_at[kSfAtomTile];
   float kx[kSfNodesPerThread], ky[kSfNodesPerThread], kz[kSfNodesPerThread];
   double Kx[kSfNodesPerThread], Ky[kSfNodesPerThread], Kz[kSfNodesPerThread];
@@ -253,7 +253,7 @@ k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ 
       double ts, tc;
       sincos(Kx[u] * cx + Ky[u] * cy + Kz[u] * cz, &ts, &tc);
       // (sr + i si) * (tc - i ts)
-      S[(size_t)cell * K + k] = make_double2(sr[u] * tc + si[u] * ts, si[u] * tc - sr[u] * ts);
+      S[(size_t)cell * ld + k] = make_double2(sr[u] * tc + si[u] * ts, si[u] * tc - sr[u] * ts);
     }
   }
 }
@@ -271,7 +271,8 @@ struct SatArgs {
   const double2 *S;
   const double4 *node64;        // (kx, ky, kz, w) FP64
   const uint32_t *node_radii;   // r_in | r_out << 16
-  uint32_t K;
+  uint32_t K;                   // nodes handled by this launch
+  uint32_t ld;                  // row stride of S and R (nodes per cell row)
   uint32_t nb;                  // nodes per CTA
   uint32_t stride;              // shared row stride (complex) = ncell + 1
   float2 *R;
@@ -330,7 +331,7 @@ k_shell_sums(Grid g, SatArgs a) {
 #pragma unroll 4
   for (uint32_t t = threadIdx.x; t < C * nb; t += blockDim.x) {
     const uint32_t c = t / nb, j = t % nb;
-    s_sat[j * a.stride + c] = a.S[(size_t)c * a.K + k0 + j];
+    s_sat[j * a.stride + c] = a.S[(size_t)c * a.ld + k0 + j];
   }
   __syncthreads();
   // prefix along z (lines indexed by node, x, y)
@@ -374,7 +375,7 @@ k_shell_sums(Grid g, SatArgs a) {
     const double2 sh = make_double2((o.x - i.x) * w, (o.y - i.y) * w);
     const double2 *tw = s_tw + j * naxis;
     const double2 r = cmul(cmul(sh, tw[x]), cmul(tw[g.nx + y], tw[g.nx + g.ny + z]));
-    a.R[(size_t)c * a.K + k] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
+    a.R[(size_t)c * a.ld + k] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
   }
 }
 

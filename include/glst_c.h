@@ -71,6 +71,7 @@ typedef struct glst_info {
   uint32_t group_r_in[16];
   uint32_t group_r_out[16];
   uint64_t device_bytes;    /* device memory held by the handle */
+  uint32_t kernels_per_compute; /* kernel launches of one glst_compute */
 } glst_info;
 
 /* Where spherical t-designs are read from.  Either the project's binary store
