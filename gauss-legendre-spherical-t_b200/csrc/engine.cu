@@ -389,7 +389,7 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
       }
       ref_base += g.n_radial * g.n_dir;
       ibase += g.n_radial * g.n_dir;
-      if (g.n_radial > (unsigned)dev::kLrTileNodes)
+      if (g.n_radial > (unsigned)dev::kLrfTileNodes)
         return fail(GLST_ERR_SIZE, "%u radial nodes exceed the tile of the long-range kernel", g.n_radial);
     }
     GLST_TRY(dalloc_n(h, &h->node32, K));
@@ -531,10 +531,10 @@ static glst_status shell_range(glst_handle *h, uint32_t kb, uint32_t ke, cudaStr
 
 static glst_status lr_range(glst_handle *h, uint32_t c0, uint32_t c1, cudaStream_t st) {
   if (c1 <= c0 || !h->plan.natom) return GLST_OK;
-  dim3 grid(h->plan.ncell, c1 - c0);
-  dev::k_long_range<<<grid, dev::kLrThreads, 0, st>>>(h->pk, h->cell_count, h->cell_point, h->chunks + c0,
-                                                      h->dirs, h->kappa, h->R, h->K, h->plan.natom,
-                                                      h->part + (size_t)c0 * h->plan.natom);
+  dim3 grid((h->plan.natom + dev::kLrThreads - 1) / dev::kLrThreads, c1 - c0);
+  dev::k_long_range_flat<<<grid, dev::kLrThreads, 0, st>>>(
+      h->pk, h->cell_point, h->plan.ncell, h->chunks + c0, h->dirs, h->kappa, h->R, h->K, h->plan.natom,
+      h->part + (size_t)c0 * h->plan.natom);
   CUDA_TRY(cudaGetLastError());
   return GLST_OK;
 }

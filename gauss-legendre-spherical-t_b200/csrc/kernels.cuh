@@ -386,13 +386,8 @@ k_shell_sums(Grid g, SatArgs a) {
 // so per atom and direction u = s_j . d_i is formed once and each node costs
 // one multiply, one SFU sin/cos pair and four FMAs:
 //   e += c R'x - s R'y,   g += kappa_r (c R'y + s R'x),   f += g s_j.
-// CTA = (cell, chunk of directions of one group); thread = atom of the cell;
-// the chunk's R' rows are prefetched into registers and staged through
-// double-buffered shared-memory tiles as (R'x, R'y, kappa_r) float4s.  FP32
-// inside a tile (at most 512 nodes), FP64 across tiles.
+// FP32 inside a tile, FP64 across tiles.
 constexpr int kLrThreads = 128;
-constexpr int kLrTileNodes = 512;   // nodes per shared tile (whole directions)
-constexpr int kLrPerThread = kLrTileNodes / kLrThreads;
 
 struct LrChunk {
   uint32_t node_begin;   // internal index of (first direction, r = 0)
@@ -403,67 +398,93 @@ struct LrChunk {
   uint32_t pad[3];
 };
 
-// Each thread loads its share of a tile's R' values into registers; stored
-// to shared memory (with kappa interleaved) after the previous tile's work.
-__device__ __forceinline__ void lr_prefetch(float2 (&pre)[kLrPerThread], const float2 *__restrict__ src,
-                                            uint32_t n) {
-#pragma unroll
-  for (int k = 0; k < kLrPerThread; k++) {
-    const uint32_t t = threadIdx.x + k * kLrThreads;
-    pre[k] = t < n ? src[t] : make_float2(0.f, 0.f);
+// A CTA takes 128 consecutive cell-ordered atoms whatever their cells (so
+// every warp is full -- one CTA per cell left ~10-15 % of the lanes of last
+// warps idle, measured 2.06 vs 1.63 ms on water10k), and stages
+// the R' tiles of the up to kLrfCells cells those atoms belong to; lanes read
+// their own cell's tile (at most a few distinct addresses per warp).  Atoms
+// of sparser ranges (more cells) are handled in several passes over windows
+// of kLrfCells cells.  Per (atom, node) pair: the arithmetic above.
+constexpr int kLrfCells = 4;          // cells staged per pass
+constexpr int kLrfTileNodes = 256;    // nodes per cell tile
+constexpr int kLrfPerThread = (kLrfCells * kLrfTileNodes) / kLrThreads;
+
+__device__ __forceinline__ uint32_t cell_of_atom(const uint32_t *__restrict__ cell_point, uint32_t ncell,
+                                                 uint32_t p) {
+  // last cell whose first atom is <= p (cells may be empty: the last such)
+  uint32_t lo = 0, hi = ncell - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (cell_point[mid] <= p) lo = mid;
+    else hi = mid - 1;
   }
+  return lo;
 }
 
-__global__ void __launch_bounds__(kLrThreads, 10)
-k_long_range(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_count,
-             const uint32_t *__restrict__ cell_point, const LrChunk *__restrict__ chunks,
-             const float4 *__restrict__ dirs, const float *__restrict__ kappa,
-             const float2 *__restrict__ R, uint32_t K, uint32_t natom, double4 *__restrict__ part) {
-  __shared__ float4 s_n[2][kLrTileNodes];  // (R'x, R'y, kappa_r, 0) per node
-  __shared__ float s_kappa[kLrTileNodes];
-  const uint32_t cell = blockIdx.x;
-  const uint32_t cnt = cell_count[cell];
-  if (cnt == 0) return;
-  const uint32_t start = cell_point[cell];
+__global__ void __launch_bounds__(kLrThreads, 8)
+k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_point, uint32_t ncell,
+                  const LrChunk *__restrict__ chunks, const float4 *__restrict__ dirs,
+                  const float *__restrict__ kappa, const float2 *__restrict__ R, uint32_t K, uint32_t natom,
+                  double4 *__restrict__ part) {
+  __shared__ float4 s_n[2][kLrfCells * kLrfTileNodes];  // per cell slot: (R'x, R'y, kappa_r, 0)
+  __shared__ float s_kappa[kLrfTileNodes];
+  __shared__ uint32_t s_range[2];
+  const uint32_t a0 = blockIdx.x * kLrThreads;
+  const uint32_t p = a0 + threadIdx.x;
+  const bool active = p < natom;
   const LrChunk ch = chunks[blockIdx.y];
   const uint32_t nr = ch.n_rad;
-  const uint32_t dirs_per_tile = max(1u, kLrTileNodes / nr);
+  const uint32_t dirs_per_tile = max(1u, kLrfTileNodes / nr);  // nr <= kLrfTileNodes (host check)
   const uint32_t ntiles = (ch.n_dir + dirs_per_tile - 1) / dirs_per_tile;
   for (uint32_t t = threadIdx.x; t < nr; t += kLrThreads) s_kappa[t] = kappa[ch.kappa_begin + t];
-  const float2 *Rc = R + (size_t)cell * K + ch.node_begin;
-  for (uint32_t a0 = 0; a0 < cnt; a0 += kLrThreads) {
-    const uint32_t ai = a0 + threadIdx.x;
-    const bool active = ai < cnt;
-    const bool warp_live = a0 + (threadIdx.x & ~31u) < cnt;
-    const float4 p = active ? pk[start + ai] : make_float4(0.f, 0.f, 0.f, 0.f);
-    double ex = 0.0, ey = 0.0, ez = 0.0, ee = 0.0;
-    float2 pre[kLrPerThread];
-    __syncthreads();  // s_kappa written; previous atom block done with s_n
-    lr_prefetch(pre, Rc, min(dirs_per_tile, ch.n_dir) * nr);
+  const uint32_t last = min(a0 + kLrThreads, natom) - 1;
+  if (threadIdx.x == 0) s_range[0] = cell_of_atom(cell_point, ncell, a0);
+  if (threadIdx.x == 1) s_range[1] = cell_of_atom(cell_point, ncell, last);
+  const uint32_t my_cell = active ? cell_of_atom(cell_point, ncell, p) : 0xffffffffu;
+  const float4 pa = active ? pk[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+  __syncthreads();
+  const uint32_t cA = s_range[0], cB = s_range[1];
+  double ex = 0.0, ey = 0.0, ez = 0.0, ee = 0.0;
+  for (uint32_t w0 = cA; w0 <= cB; w0 += kLrfCells) {
+    const uint32_t nc = min((uint32_t)kLrfCells, cB - w0 + 1);
+    const bool mine = active && my_cell >= w0 && my_cell < w0 + nc;
+    const uint32_t slot = mine ? my_cell - w0 : 0;
+    const bool warp_live = __any_sync(0xffffffffu, mine);
+    float2 pre[kLrfPerThread];
+    // prefetch tile 0 of every cell of this window
+    auto prefetch = [&](uint32_t d0) {
+      const uint32_t nd = min(dirs_per_tile, ch.n_dir - d0);
+#pragma unroll
+      for (int k = 0; k < kLrfPerThread; k++) {
+        const uint32_t t = threadIdx.x + k * kLrThreads;
+        const uint32_t c = t / kLrfTileNodes, i = t % kLrfTileNodes;
+        pre[k] = (c < nc && i < nd * nr)
+                     ? R[(size_t)(w0 + c) * K + ch.node_begin + (size_t)d0 * nr + i]
+                     : make_float2(0.f, 0.f);
+      }
+    };
+    __syncthreads();  // previous window done with s_n; s_kappa visible after the next barrier
+    prefetch(0);
     for (uint32_t tile = 0; tile < ntiles; tile++) {
       const uint32_t d0 = tile * dirs_per_tile;
       const uint32_t nd = min(dirs_per_tile, ch.n_dir - d0);
       float4 *buf = s_n[tile & 1];
 #pragma unroll
-      for (int k = 0; k < kLrPerThread; k++) {
+      for (int k = 0; k < kLrfPerThread; k++) {
         const uint32_t t = threadIdx.x + k * kLrThreads;
-        if (t < nd * nr) buf[t] = make_float4(pre[k].x, pre[k].y, s_kappa[t % nr], 0.f);
+        const uint32_t i = t % kLrfTileNodes;
+        if (t / kLrfTileNodes < nc && i < nd * nr) buf[t] = make_float4(pre[k].x, pre[k].y, s_kappa[i % nr], 0.f);
       }
       __syncthreads();
-      if (tile + 1 < ntiles) {
-        const uint32_t d1 = d0 + dirs_per_tile;
-        lr_prefetch(pre, Rc + (size_t)d1 * nr, min(dirs_per_tile, ch.n_dir - d1) * nr);
-      }
+      if (tile + 1 < ntiles) prefetch(d0 + dirs_per_tile);
       if (warp_live) {
         float tx = 0.f, ty = 0.f, tz = 0.f, te = 0.f;
+        const float4 *cb = buf + slot * kLrfTileNodes;
         for (uint32_t d = 0; d < nd; d++) {
           const float4 sj = dirs[ch.dir_begin + d0 + d];
-          const float u = fmaf(sj.x, p.x, fmaf(sj.y, p.y, sj.z * p.z));
-          // Two accumulator sets (even / odd r) and split energy terms keep
-          // the FMA dependency chains short, so a warp is not limited by
-          // accumulator latency before the SFU pipe is full.
+          const float u = fmaf(sj.x, pa.x, fmaf(sj.y, pa.y, sj.z * pa.z));
           float ea = 0.f, eb = 0.f, ec = 0.f, ed = 0.f, ga = 0.f, gb = 0.f;
-          const float4 *nn = buf + d * nr;
+          const float4 *nn = cb + d * nr;
           uint32_t r = 0;
 #pragma unroll 2
           for (; r + 1 < nr; r += 2) {
@@ -492,16 +513,19 @@ k_long_range(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_co
           ty = fmaf(gsum, sj.y, ty);
           tz = fmaf(gsum, sj.z, tz);
         }
-        ee += te;
-        ex += tx;
-        ey += ty;
-        ez += tz;
+        if (mine) {
+          ee += te;
+          ex += tx;
+          ey += ty;
+          ez += tz;
+        }
       }
+      __syncthreads();
     }
-    if (active) {
-      const double q = static_cast<double>(p.w);
-      part[(size_t)blockIdx.y * natom + start + ai] = make_double4(q * ex, q * ey, q * ez, q * ee);
-    }
+  }
+  if (active) {
+    const double q = static_cast<double>(pa.w);
+    part[(size_t)blockIdx.y * natom + p] = make_double4(q * ex, q * ey, q * ez, q * ee);
   }
 }
 

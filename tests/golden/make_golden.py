@@ -38,10 +38,10 @@ CASES = {
     "w1000_tol1e-4": (1000, 31.04, 8.0, 1e-4, 3),
     "w2000_tol1e-5": (2000, 39.1, 10.0, 1e-5, 5),
     "water10k": (10000, 66.9, 10.0, math.erfc(0.31 * 10.0) / 10.0, 0),
-    # one million atoms; stored as a seeded subset of atoms plus
+    # water333k: one million atoms; stored as a seeded subset of atoms plus
     # digests of the full assignment (the full arrays would be 36 MB)
     "water333k": (333333, 215.3, 10.0, math.erfc(0.31 * 10.0) / 10.0, 0),
-    # configs[1] at the next higher cubature order (tol / 10)
+    # water10k at the next higher cubature order (tol / 10)
     "water10k_next": (10000, 66.9, 10.0, math.erfc(0.31 * 10.0) / 100.0, 0),
 }
 SUBSET = {"water333k": 20000}

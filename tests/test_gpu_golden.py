@@ -44,7 +44,7 @@ def test_cuda_path_matches_reference(pkg, case, ct):
 
 
 def test_water333k_matches_reference_subset(pkg):
-    """333,333 waters (999,999 atoms), L = 215.3 A.  The fixture
+    """water333k: 333,333 waters (999,999 atoms), L = 215.3 A.  The fixture
     holds the reference's outputs on a seeded subset of 20,000 atoms, its
     total energy, and a digest of its full cell assignment."""
     import hashlib
@@ -71,7 +71,7 @@ def test_water333k_matches_reference_subset(pkg):
 
 
 def test_water10k_next_order_matches_reference(pkg):
-    """configs[1] at the next higher cubature order (tol/10: t = 101, 83, 57,
+    """water10k at the next higher cubature order (tol/10: t = 101, 83, 57,
     K = 192,478 nodes) against the reference's glst_force<double>."""
     d, (x, y, z, q), box = load_case("water10k_next", "double")
     dev = [torch.tensor(a, dtype=torch.float64, device="cuda:0") for a in (x, y, z, q)]

@@ -77,7 +77,7 @@ def test_far_field_parity(pkg, store, name):
 
 
 def test_water216_matches_direct_coulomb(pkg, store):
-    """216 waters, L = 18.63 A, rcut 9, alpha 0.34.  All atoms sit
+    """water216: 216 waters, L = 18.63 A, rcut 9, alpha 0.34.  All atoms sit
     in cells 0..1 of the 3x3x3 grid, so the far field is empty and GLST equals
     the direct sum."""
     from glst_b200 import systems
@@ -256,7 +256,7 @@ def test_dense_cell_overflow_is_reported(pkg):
 
 @pytest.mark.slow
 def test_water10k_parity(pkg, store):
-    """configs[1] workload: 10,000 waters, L = 66.9 A, rcut 10, alpha 0.31."""
+    """water10k workload: 10,000 waters, L = 66.9 A, rcut 10, alpha 0.31."""
     from glst_b200 import systems
     s = systems.config_system("water10k", seed=0)
     L = s["box"][0]
