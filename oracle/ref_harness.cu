@@ -13,6 +13,7 @@
 // directory where that folder holds the project-generated designs.
 //
 // usage: glst_ref_harness <in.bin> <out.bin> <float|double> <iterations>
+//        glst_ref_harness --batch <list.bin> <out.bin> <float|double> <iterations>
 //   in.bin : u32 natom, f64 tol, f64 box[3], f64 rcut, f64 x[N], y[N], z[N], q[N]
 //   out.bin: u32 natom, u32 K, u32 nx, ny, nz, u32 iterations,
 //            f64 ms_mean[8] (assign, sf, sum, lr, sr, comm, total, events_total),
@@ -117,7 +118,105 @@ static int run(const char *out_path, unsigned natom, double tol,
   return 0;
 }
 
+// Batch mode: the reference's plain path on many independent systems, one
+// after another (construct, one warm-up solve, `iters` timed solves, get_ef,
+// destroy).  Only calc_ener_force is timed, the same host-clock-plus-sync
+// method as above.
+//   list.bin: u32 nsys, then per system the in.bin record above
+//   out.bin : u32 nsys, then per system u32 natom, u32 K, f64 ms_host,
+//             f64 ms_events, f64 energy (0.5 * sum en)
+template <typename CT>
+static int run_batch(FILE *in, FILE *out, unsigned nsys, int iters) {
+  std::fwrite(&nsys, sizeof(unsigned), 1, out);
+  for (unsigned s = 0; s < nsys; s++) {
+    unsigned natom = 0;
+    double tol = 0, box[3] = {0, 0, 0}, rcut = 0;
+    if (std::fread(&natom, sizeof(unsigned), 1, in) != 1) return 2;
+    if (std::fread(&tol, sizeof(double), 1, in) != 1) return 2;
+    if (std::fread(box, sizeof(double), 3, in) != 3) return 2;
+    if (std::fread(&rcut, sizeof(double), 1, in) != 1) return 2;
+    std::vector<double> x(natom), y(natom), z(natom), q(natom);
+    for (auto *v : {&x, &y, &z, &q})
+      if (std::fread(v->data(), sizeof(double), natom, in) != natom) return 2;
+    double ms_host = 0, ms_ev = 0, energy = 0;
+    unsigned K = 0;
+    {
+      cuda_container<double> rx(x), ry(y), rz(z), qc(q);
+      rx.transfer_to_device();
+      ry.transfer_to_device();
+      rz.transfer_to_device();
+      qc.transfer_to_device();
+      glst_force<CT> glst(natom, tol, box[0], box[1], box[2], rcut);
+      K = glst.cubature_ ? glst.cubature_->tot_num_nodes() : 0u;
+      cudaEvent_t e0, e1;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      for (int it = -1; it < iters; it++) {
+        glst.fx()[0].set(0.0);
+        glst.fy()[0].set(0.0);
+        glst.fz()[0].set(0.0);
+        glst.en()[0].set(0.0);
+        cudaDeviceSynchronize();
+        cudaEventRecord(e0, 0);
+        auto t0 = std::chrono::high_resolution_clock::now();
+        glst.calc_ener_force(rx.d_array().data(), ry.d_array().data(),
+                             rz.d_array().data(), qc.d_array().data());
+        cudaDeviceSynchronize();
+        auto t1 = std::chrono::high_resolution_clock::now();
+        cudaEventRecord(e1, 0);
+        cudaEventSynchronize(e1);
+        float evms = 0.f;
+        cudaEventElapsedTime(&evms, e0, e1);
+        if (it >= 0) {
+          ms_host += std::chrono::duration<double, std::milli>(t1 - t0).count();
+          ms_ev += evms;
+        }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      cuda_container<double> fx, fy, fz, en;
+      glst.get_ef(fx, fy, fz, en);
+      for (unsigned i = 0; i < natom; i++) energy += en.h_array()[i];
+      energy *= 0.5;
+    }
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) {
+      std::fprintf(stderr, "CUDA error: %s\n", cudaGetErrorString(err));
+      return 3;
+    }
+    const double div = iters > 0 ? iters : 1;
+    ms_host /= div;
+    ms_ev /= div;
+    std::fwrite(&natom, sizeof(unsigned), 1, out);
+    std::fwrite(&K, sizeof(unsigned), 1, out);
+    std::fwrite(&ms_host, sizeof(double), 1, out);
+    std::fwrite(&ms_ev, sizeof(double), 1, out);
+    std::fwrite(&energy, sizeof(double), 1, out);
+  }
+  return 0;
+}
+
 int main(int argc, char **argv) {
+  if (argc == 6 && std::string(argv[1]) == "--batch") {
+    FILE *in = std::fopen(argv[2], "rb");
+    if (!in) return 2;
+    FILE *out = std::fopen(argv[3], "wb");
+    if (!out) return 2;
+    unsigned nsys = 0;
+    if (std::fread(&nsys, sizeof(unsigned), 1, in) != 1) return 2;
+    int rc = 0;
+    try {
+      rc = std::string(argv[4]) == "float"
+               ? run_batch<float>(in, out, nsys, std::atoi(argv[5]))
+               : run_batch<double>(in, out, nsys, std::atoi(argv[5]));
+    } catch (const std::exception &e) {
+      std::fprintf(stderr, "reference threw: %s\n", e.what());
+      rc = 4;
+    }
+    std::fclose(in);
+    std::fclose(out);
+    return rc;
+  }
   if (argc != 5) {
     std::fprintf(stderr, "usage: %s in.bin out.bin float|double iterations\n",
                  argv[0]);

@@ -13,7 +13,9 @@ nodes.
 
     python tests/golden/make_golden.py [case ...]
 
-Output: tests/golden/<case>_<ct>.npz, plus a timing summary on stdout.
+Output: tests/golden/<case>_<ct>.npz, plus a timing summary on stdout.  The
+case ``batch256`` runs the 256-system uneven batch through the reference one
+system after another and keeps per-system energies and solve times.
 """
 import json
 import math
@@ -105,6 +107,47 @@ def render_tdesigns(dst):
     make_tdesigns.write_reference_dir(g.TDESIGN_STORE, os.path.join(dst, "SS31-Mar-2016"))
 
 
+# The uneven batch: 256 independent water boxes (300-30,000 atoms, two cubature
+# orders, seed 0), run by the reference one system after another (its plain
+# path).  The fixture keeps each system's total energy and solve time.
+BATCH_CASE = "batch256"
+
+
+def batch_inputs_sha256(sy):
+    return input_sha256(*[np.concatenate([s[k] for s in sy]) for k in ("x", "y", "z", "q")])
+
+
+def make_batch(work, iters=2):
+    from glst_b200 import systems
+    sy = systems.batch_uneven(256, seed=0)
+    lst = os.path.join(work, "batch.in")
+    with open(lst, "wb") as f:
+        f.write(struct.pack("<I", len(sy)))
+    for s in sy:
+        rec = lst + ".one"
+        write_input(rec, s["x"], s["y"], s["z"], s["q"], s["tol"], s["box"][0], s["rcut"])
+        with open(lst, "ab") as f, open(rec, "rb") as g:
+            f.write(g.read())
+    out = os.path.join(work, "batch.out")
+    r = subprocess.run([harness(), "--batch", lst, out, "double", str(iters)], cwd=work, capture_output=True,
+                       text=True)
+    if r.returncode != 0:
+        print(r.stdout[-2000:], r.stderr[-2000:])
+        raise SystemExit("reference harness failed on the batch (%d)" % r.returncode)
+    with open(out, "rb") as f:
+        data = f.read()
+    (nsys,) = struct.unpack_from("<I", data, 0)
+    rec = np.dtype([("natom", "<u4"), ("K", "<u4"), ("ms_host", "<f8"), ("ms_events", "<f8"), ("energy", "<f8")])
+    o = np.frombuffer(data, dtype=rec, count=nsys, offset=4)
+    np.savez_compressed(os.path.join(HERE, BATCH_CASE + "_double.npz"), natom=o["natom"].copy(), K=o["K"].copy(),
+                        ms_host=o["ms_host"].copy(), ms_events=o["ms_events"].copy(), energy=o["energy"].copy(),
+                        tol=np.array([s["tol"] for s in sy]), input_sha256=np.array(batch_inputs_sha256(sy)))
+    summary = dict(systems=int(nsys), atoms=int(o["natom"].sum()), sequential_ms_host=float(o["ms_host"].sum()),
+                   sequential_ms_events=float(o["ms_events"].sum()))
+    print(json.dumps({BATCH_CASE + "_double": summary}), flush=True)
+    return summary
+
+
 def main(cases, iters=3):
     g = __graft_entry__.load_package()
     from glst_b200 import systems
@@ -114,6 +157,9 @@ def main(cases, iters=3):
     with tempfile.TemporaryDirectory() as work:
         render_tdesigns(work)
         for case in cases:
+            if case == BATCH_CASE:
+                summary[case] = make_batch(work)
+                continue
             n_mol, L, rcut, tol, seed = CASES[case]
             x, y, z, q = systems.water_box(n_mol, L, seed=seed)
             digest = input_sha256(x, y, z, q)
@@ -151,4 +197,4 @@ def main(cases, iters=3):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or list(CASES))
+    main(sys.argv[1:] or list(CASES) + [BATCH_CASE])

@@ -44,3 +44,31 @@ def test_batch_equals_individual_solves(pkg):
         for a, g in zip(alone, graph):
             assert np.array_equal(a, g[off[i]:off[i + 1]]), i
         assert e == e_graph[i]
+
+
+def test_batch256_energies_match_reference(pkg):
+    """The 256-system uneven batch (300-30,000 atoms, two cubature orders),
+    solved in one captured graph, against the reference library run on the
+    same systems one after another: every system's total energy within 1e-7
+    relative.  Fixture: tests/golden/batch256_double.npz (make_golden.py)."""
+    import os
+    from glst_b200 import systems as S
+    path = os.path.join(os.path.dirname(__file__), "golden", "batch256_double.npz")
+    if not os.path.exists(path):
+        pytest.skip("batch256 fixture not generated")
+    gold = np.load(path)
+    sy = S.batch_uneven(256, seed=0)
+    import hashlib
+    digest = hashlib.sha256(b"".join(np.ascontiguousarray(np.concatenate([s[k] for s in sy]), dtype="<f8").tobytes()
+                                     for k in ("x", "y", "z", "q"))).hexdigest()
+    assert str(gold["input_sha256"]) == digest
+    ins = [_cat(sy, k) for k in ("x", "y", "z", "q")]
+    n = ins[0].numel()
+    outs = [torch.empty(n, dtype=torch.float64, device="cuda:0") for _ in range(4)]
+    with pkg.GlstBatch(sy, nstreams=16) as b:
+        b.compute(*ins, *outs)
+        e = b.energies()
+    ref = gold["energy"]
+    assert np.array_equal(gold["natom"], [s["natom"] for s in sy])
+    rel = np.abs(e - ref) / np.abs(ref)
+    assert rel.max() <= 1e-7, (int(rel.argmax()), float(rel.max()))
