@@ -212,10 +212,19 @@ def run_batch(g, torch, dev, stream, n_steps=4, n_sys=256, seed=0):
     b.close()
     del ins, outs
     torch.cuda.empty_cache()
-    return {"workload": "%d uneven water boxes, %d atoms (300-30,000 each), 2 cubature orders" % (n_sys, n),
-            "unit": UNIT, "batched": res["batched"], "plain": res["plain"],
-            "ratio": res["plain"]["ms_per_step"] / res["batched"]["ms_per_step"],
-            "create_s": t_create, "steps": n_steps}
+    out = {"workload": "%d uneven water boxes, %d atoms (300-30,000 each), 2 cubature orders" % (n_sys, n),
+           "unit": UNIT, "batched": res["batched"], "plain": res["plain"],
+           "ratio": res["plain"]["ms_per_step"] / res["batched"]["ms_per_step"],
+           "create_s": t_create, "steps": n_steps}
+    # The reference library's plain path on the same 256 systems (one solve
+    # after another, calc_ener_force only), recorded on a B200 with the
+    # reference harness into the batch256 golden fixture.
+    gold = os.path.join(ROOT, "tests", "golden", "batch256_double.npz")
+    if n_sys == 256 and seed == 0 and os.path.exists(gold):
+        ref_ms = float(np.load(gold)["ms_host"].sum())
+        out["reference_plain_recorded"] = {"ms_per_step": ref_ms, "value": n / (ref_ms * 1e-3),
+                                           "batched_ratio": ref_ms / res["batched"]["ms_per_step"]}
+    return out
 
 
 def run_serve(g, n_requests=120, loads=(0.5, 0.8, 1.1), budget=150 << 30, nslots=8, seed=0):
