@@ -138,12 +138,14 @@ struct glst_handle {
   float4 *pk = nullptr;
   double4 *pd = nullptr;
   // nodes, internal order: group -> direction -> radial
-  float4 *node32 = nullptr;
   double4 *node64 = nullptr;
   uint32_t *node_radii = nullptr;
   float4 *dirs = nullptr;       // unit directions, FP32
   float *kappa = nullptr;       // radial scales per group, FP32
   dev::LrChunk *chunks = nullptr;
+  dev::SfUnit *sf_units = nullptr;  // structure-factor work units (whole directions)
+  size_t sf_unit_bytes = 0;
+  uint32_t n_sf_units = 0;
   // far field
   double2 *S = nullptr;
   float2 *R = nullptr;
@@ -160,6 +162,7 @@ struct glst_handle {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_far2 = nullptr;
   struct FarRange {
     uint32_t kb, ke, c0, c1;  // nodes and long-range chunks of one pipeline stage
+    uint32_t u0, u1;          // structure-factor units of the same nodes
   };
   std::vector<FarRange> ranges;
 };
@@ -206,8 +209,10 @@ static void release(glst_handle *h) {
   h->bufs.clear();
   h->pending.clear();
   if (h->chunks) cudaFree(h->chunks);
+  if (h->sf_units) cudaFree(h->sf_units);
   if (h->part) cudaFree(h->part);
   h->chunks = nullptr;
+  h->sf_units = nullptr;
   h->part = nullptr;
   h->part_cap = 0;
   h->bytes = 0;
@@ -299,21 +304,66 @@ static glst_status build_chunks(glst_handle *h) {
       if (s + 1 == stages) c1 = h->nsplit;
       const uint32_t kb = chunks[c0].node_begin;
       const uint32_t ke = chunks[c1 - 1].node_begin + chunks[c1 - 1].n_dir * chunks[c1 - 1].n_rad;
-      h->ranges.push_back({kb, ke, c0, c1});
+      h->ranges.push_back({kb, ke, c0, c1, 0, 0});
       c0 = c1;
     }
   }
+  // Structure-factor units: per stage, each group's run of directions (its
+  // chunks are contiguous) cut into units of kSfThreads / nb directions, nb
+  // threads per direction of npt <= kSfMaxNpt radial nodes.  Cutting the
+  // group's whole run, not each long-range chunk, keeps the units full.
+  std::vector<dev::SfUnit> units;
+  for (auto &rg : h->ranges) {
+    rg.u0 = (uint32_t)units.size();
+    for (uint32_t ci = rg.c0; ci < rg.c1;) {
+      const auto &c = chunks[ci];
+      uint32_t n_dir = c.n_dir, cj = ci + 1;
+      while (cj < rg.c1 && chunks[cj].kappa_begin == c.kappa_begin && chunks[cj].dir_begin == c.dir_begin + n_dir) {
+        n_dir += chunks[cj].n_dir;
+        cj++;
+      }
+      const uint32_t nb = (c.n_rad + dev::kSfMaxNpt - 1) / dev::kSfMaxNpt;
+      const uint32_t npt = (c.n_rad + nb - 1) / nb;
+      const uint32_t dpu = dev::kSfThreads / nb;
+      for (uint32_t j0 = 0; j0 < n_dir; j0 += dpu) {
+        dev::SfUnit u{};
+        u.node_begin = c.node_begin + j0 * c.n_rad;
+        u.dir_begin = c.dir_begin + j0;
+        u.n_dir = std::min(dpu, n_dir - j0);
+        u.n_rad = c.n_rad;
+        u.nb = nb;
+        u.npt = npt;
+        u.kappa_begin = c.kappa_begin;
+        units.push_back(u);
+      }
+      ci = cj;
+    }
+    rg.u1 = (uint32_t)units.size();
+  }
+  h->n_sf_units = (uint32_t)units.size();
+  if (units.size() > 0x7FFFFFFFu) return fail(GLST_ERR_SIZE, "too many structure-factor units");
   if (h->chunks) {
     cudaFree(h->chunks);
     h->bytes -= h->chunk_bytes;
   }
   h->chunks = nullptr;
+  h->sf_units = nullptr;
   h->chunk_bytes = 0;
+  if (h->sf_units) {
+    cudaFree(h->sf_units);
+    h->bytes -= h->sf_unit_bytes;
+  }
+  h->sf_units = nullptr;
+  h->sf_unit_bytes = 0;
   if (!chunks.empty()) {
     h->chunk_bytes = chunks.size() * sizeof(dev::LrChunk);
     CUDA_TRY(cudaMalloc(&h->chunks, h->chunk_bytes));
     h->bytes += h->chunk_bytes;
     CUDA_TRY(cudaMemcpy(h->chunks, chunks.data(), h->chunk_bytes, cudaMemcpyHostToDevice));
+    h->sf_unit_bytes = units.size() * sizeof(dev::SfUnit);
+    CUDA_TRY(cudaMalloc(&h->sf_units, h->sf_unit_bytes));
+    h->bytes += h->sf_unit_bytes;
+    CUDA_TRY(cudaMemcpy(h->sf_units, units.data(), h->sf_unit_bytes, cudaMemcpyHostToDevice));
   }
   if ((size_t)h->nsplit > h->part_cap) {
     if (h->part) {
@@ -359,7 +409,6 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
   // Nodes and weights are rounded to CT first, as the reference stores them
   // (src/cubature.cu:138-141).
   std::vector<uint32_t> kappa_base, dir_base, node_base;
-  std::vector<float4> n32(K);
   std::vector<double4> n64(K);
   std::vector<uint32_t> radii(K);
   std::vector<float4> dirs;
@@ -383,7 +432,6 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
             kx = (double)(float)kx; ky = (double)(float)ky; kz = (double)(float)kz; w = (double)(float)w;
           }
           n64[k] = make_double4(kx, ky, kz, w);
-          n32[k] = make_float4((float)kx, (float)ky, (float)kz, 0.f);
           radii[k] = (g.r_in & 0xffffu) | (g.r_out << 16);
         }
       }
@@ -392,7 +440,6 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
       if (g.n_radial > (unsigned)dev::kLrfTileNodes)
         return fail(GLST_ERR_SIZE, "%u radial nodes exceed the tile of the long-range kernel", g.n_radial);
     }
-    GLST_TRY(dalloc_n(h, &h->node32, K));
     GLST_TRY(dalloc_n(h, &h->node64, K));
     GLST_TRY(dalloc_n(h, &h->node_radii, K));
     GLST_TRY(dalloc_n(h, &h->dirs, dirs.size()));
@@ -458,7 +505,6 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
   }
   GLST_TRY(commit_allocs(h));
   if (K) {
-    CUDA_TRY(cudaMemcpy(h->node32, n32.data(), K * sizeof(float4), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(h->node64, n64.data(), K * sizeof(double4), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(h->node_radii, radii.data(), K * sizeof(uint32_t), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(h->dirs, dirs.data(), dirs.size() * sizeof(float4), cudaMemcpyHostToDevice));
@@ -504,17 +550,17 @@ static glst_status phase_assign(glst_handle *h, const double *rx, const double *
   return GLST_OK;
 }
 
-// Far-field phases over a range of the handle's nodes [kb, ke) (local,
-// internal order) and of its long-range chunks [c0, c1).
-static glst_status sf_range(glst_handle *h, uint32_t kb, uint32_t ke, cudaStream_t st) {
-  if (ke <= kb || !h->plan.natom) return GLST_OK;
-  const uint32_t per = dev::kSfThreads * dev::kSfNodesPerThread;
+// Far-field phases over a range of the handle's nodes (local, internal
+// order): structure-factor units [u0, u1), shell sums over nodes [kb, ke),
+// long-range chunks [c0, c1).
+static glst_status sf_range(glst_handle *h, uint32_t u0, uint32_t u1, cudaStream_t st) {
+  if (u1 <= u0 || !h->plan.natom) return GLST_OK;
   const uint32_t cg = (h->plan.ncell + dev::kSfCellsPerCta - 1) / dev::kSfCellsPerCta;
   if (cg > 65535) return fail(GLST_ERR_SIZE, "too many cells for the structure-factor grid");
-  dim3 grid((ke - kb + per - 1) / per, cg);
-  dev::k_structure_factors<<<grid, dev::kSfThreads, 0, st>>>(
-      h->pk, h->cell_count, h->cell_point, h->grid, h->node32 + h->k_begin + kb, h->node64 + h->k_begin + kb,
-      ke - kb, h->K, h->S + kb);
+  dim3 grid(u1 - u0, cg);
+  dev::k_structure_factors<<<grid, dev::kSfThreads, 0, st>>>(h->pk, h->cell_count, h->cell_point, h->grid,
+                                                              h->sf_units + u0, h->dirs, h->kappa,
+                                                              h->node64 + h->k_begin, h->K, h->S);
   CUDA_TRY(cudaGetLastError());
   return GLST_OK;
 }
@@ -540,7 +586,7 @@ static glst_status lr_range(glst_handle *h, uint32_t c0, uint32_t c1, cudaStream
 }
 
 static glst_status phase_sf(glst_handle *h, cudaStream_t st) {
-  return h->K ? sf_range(h, 0, h->K, st) : GLST_OK;
+  return h->K ? sf_range(h, 0, h->n_sf_units, st) : GLST_OK;
 }
 
 static glst_status phase_shell(glst_handle *h, cudaStream_t st) {
@@ -595,7 +641,7 @@ static glst_status compute_all(glst_handle *h, const double *rx, const double *r
     for (size_t r = 0; r < h->ranges.size(); r++) {
       const auto &rg = h->ranges[r];
       cudaStream_t s = (r & 1) ? h->far2 : st;
-      GLST_TRY(sf_range(h, rg.kb, rg.ke, s));
+      GLST_TRY(sf_range(h, rg.u0, rg.u1, s));
       GLST_TRY(shell_range(h, rg.kb, rg.ke, s));
       GLST_TRY(lr_range(h, rg.c0, rg.c1, s));
     }
@@ -1286,7 +1332,7 @@ uint64_t estimate_bytes(const Plan &p, int nsm) {
   if (K) {
     const uint64_t slots = (uint64_t)nsm * 16;
     const uint64_t chunks = std::max<uint64_t>(1, (8 * slots + C - 1) / C) + p.groups.size() + 1;
-    b += K * (16 + 32 + 4 + 16 + 4) + C * K * (16 + 8) + chunks * N * 32;
+    b += K * (32 + 4 + 16 + 4) + C * K * (16 + 8) + chunks * N * 32;
   }
   return b + 64 * 16 * 64;  // per-buffer allocation granularity
 }

@@ -186,76 +186,179 @@ __global__ void k_sort_pack(const uint32_t *__restrict__ perm,
 }
 
 // ----------------------------------------------------------------------------
+// Sine and cosine on the FP32 FMA pipe, for part of the (atom, node) pairs so
+// that the FMA pipe carries some of the work the MUFU pipe would otherwise
+// serialise.  Method: theta = n pi + r with n = rint(theta / pi) (rounded by
+// adding 1.5 * 2^23), r = theta - n pi in two FMA steps (pi = kPiHi + kPiLo,
+// kPiHi with 8 significant bits so n * kPiHi is exact), then
+//   sin r = r + r^3 P(r^2),  cos r = Q(r^2)   on |r| <= pi/2,
+// with P of degree 3 and Q of degree 4, coefficients fitted by this project
+// (Lawson-weighted least squares on [0, (pi/2)^2], csrc/fit_sincos.py).
+// sin(theta) = (-1)^n sin r, cos(theta) = (-1)^n cos r: the common sign is
+// returned folded into a factor (the atom's charge) instead of applied to
+// both results.  Max abs error 1.8e-7 for |theta| <= 30.
+constexpr float kInvPi = 0.318309886183790672f;
+constexpr float kRoundMagic = 12582912.0f;  // 1.5 * 2^23
+constexpr float kPiHi = 3.140625f;
+constexpr float kPiLo = 9.67653589793e-4f;
+constexpr float kSin1 = -0.16666658222675323f, kSin2 = 0.008333051577210426f,
+                kSin3 = -0.000198090827325359f, kSin4 = 2.6052375687868334e-06f;
+constexpr float kCos0 = 0.9999999403953552f, kCos1 = -0.4999990463256836f, kCos2 = 0.04166358709335327f,
+                kCos3 = -0.0013853712007403374f, kCos4 = 2.3154068912845105e-05f;
+
+__device__ __forceinline__ void fma_sincos_signed(float th, float q, float *s, float *c, float *qs) {
+  const float t = fmaf(th, kInvPi, kRoundMagic);
+  const float n = t - kRoundMagic;
+  float r = fmaf(-n, kPiHi, th);
+  r = fmaf(-n, kPiLo, r);
+  const float r2 = r * r;
+  float p = fmaf(kSin4, r2, kSin3);
+  p = fmaf(p, r2, kSin2);
+  p = fmaf(p, r2, kSin1);
+  *s = fmaf(p * r2, r, r);
+  float cc = fmaf(kCos4, r2, kCos3);
+  cc = fmaf(cc, r2, kCos2);
+  cc = fmaf(cc, r2, kCos1);
+  *c = fmaf(cc, r2, kCos0);
+  *qs = __int_as_float(__float_as_int(q) ^ (__float_as_int(t) << 31));
+}
+
+// ----------------------------------------------------------------------------
 // Structure factors.  S_c(k) = sum_{j in c} q_j e^{-i k.r_j}
 //                            = e^{-i k.c} sum_j q_j e^{-i k.d_j},  d_j = r_j - c.
-// The inner sum runs in FP32 on cell-relative coordinates (|k.d| <~ 25 rad,
-// SFU sincos); the twiddle e^{-ik.c} and the result are FP64.
-// CTA: 128 threads x 2 nodes; loops over kCellsPerCta consecutive cells.
+// Nodes are k = kappa_r s (group -> direction -> radial), so per atom and
+// direction u = s.d_j is formed once and each node's phase is one multiply.
+// A CTA takes one work unit -- up to 128 / nb directions of one group, nb
+// threads per direction, each thread NPT consecutive radial nodes -- and
+// kSfCellsPerCta consecutive cells.  Per (atom, node): one multiply, a sine
+// and cosine (SFU, or the FMA-pipe polynomial for the last NPOLY slots), two
+// FMAs.  FP32 over a tile of <= kSfAtomTile atoms (|k.d| <~ 25 rad), then
+// FP64: the twiddle e^{-ik.c} and the sum over tiles.
 constexpr int kSfThreads = 128;
-constexpr int kSfNodesPerThread = 2;
-constexpr int kSfCellsPerCta = 8;
+constexpr int kSfMaxNpt = 12;     // radial nodes per thread, at most
+constexpr int kSfCellsPerCta = 2;
 constexpr int kSfAtomTile = 128;
 
-__global__ void __launch_bounds__(kSfThreads)
-k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_count,
-                    const uint32_t *__restrict__ cell_point, Grid g,
-                    const float4 *__restrict__ node32, const double4 *__restrict__ node64,
-                    uint32_t K, uint32_t ld, double2 *__restrict__ S) {
-  __shared__ float4 s_at[kSfAtomTile];
-  float kx[kSfNodesPerThread], ky[kSfNodesPerThread], kz[kSfNodesPerThread];
-  double Kx[kSfNodesPerThread], Ky[kSfNodesPerThread], Kz[kSfNodesPerThread];
-  bool act[kSfNodesPerThread];
-#pragma unroll
-  for (int u = 0; u < kSfNodesPerThread; u++) {
-    const uint32_t k = blockIdx.x * (kSfThreads * kSfNodesPerThread) + u * kSfThreads + threadIdx.x;
-    act[u] = k < K;
-    const float4 a = act[u] ? node32[k] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const double4 b = act[u] ? node64[k] : make_double4(0., 0., 0., 0.);
-    kx[u] = a.x; ky[u] = a.y; kz[u] = a.z;
-    Kx[u] = b.x; Ky[u] = b.y; Kz[u] = b.z;
+struct SfUnit {
+  uint32_t node_begin;   // local internal index of (first direction, r = 0)
+  uint32_t dir_begin;    // global direction index of the first direction
+  uint32_t n_dir;        // directions in the unit (<= kSfThreads / nb)
+  uint32_t n_rad;        // radial nodes per direction in this group
+  uint32_t nb;           // threads per direction
+  uint32_t npt;          // radial nodes per thread (nb * npt >= n_rad)
+  uint32_t kappa_begin;  // offset of this group's radial table
+  uint32_t pad;
+};
+
+// FMA-pipe share: about 20 % of the slots (measured on water10k: 1.49 ms
+// with none, 1.34 ms at 20 %, 1.42 ms at 30 %, 1.49 ms at 45 %).
+__host__ __device__ constexpr int sf_poly_slots(int npt) { return (2 * npt + 5) / 10; }
+
+template <int NPT>
+__device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restrict__ pk,
+                                        const uint32_t *__restrict__ cell_count,
+                                        const uint32_t *__restrict__ cell_point, const Grid &g,
+                                        const float4 *__restrict__ dirs, const float *__restrict__ kappa,
+                                        const double4 *__restrict__ node64, uint32_t ld, uint32_t c0,
+                                        uint32_t c1, double2 *__restrict__ S, float4 *s_at, float2 *s_f) {
+  constexpr int NPOLY = sf_poly_slots(NPT);
+  const uint32_t d = threadIdx.x / u.nb;
+  const uint32_t b = threadIdx.x - d * u.nb;
+  const bool act = d < u.n_dir;
+  const uint32_t r0 = b * NPT;
+  float sx = 0.f, sy = 0.f, sz = 0.f;
+  if (act) {
+    const float4 sd = dirs[u.dir_begin + d];
+    sx = sd.x; sy = sd.y; sz = sd.z;
   }
-  const uint32_t c0 = blockIdx.y * kSfCellsPerCta;
-  const uint32_t c1 = min(g.ncell, c0 + kSfCellsPerCta);
+  float kap[NPT];
+#pragma unroll
+  for (int i = 0; i < NPT; i++) kap[i] = (act && r0 + i < u.n_rad) ? kappa[u.kappa_begin + r0 + i] : 0.f;
+  const uint32_t nodes = u.n_dir * u.n_rad;
   for (uint32_t cell = c0; cell < c1; cell++) {
     const uint32_t cnt = cell_count[cell];
     const uint32_t start = cell_point[cell];
-    double sr[kSfNodesPerThread], si[kSfNodesPerThread];
-#pragma unroll
-    for (int u = 0; u < kSfNodesPerThread; u++) { sr[u] = 0.0; si[u] = 0.0; }
-    for (uint32_t a0 = 0; a0 < cnt; a0 += kSfAtomTile) {
+    const uint32_t ix = cell / (g.ny * g.nz), iy = (cell / g.nz) % g.ny, iz = cell % g.nz;
+    const double cx = cell_centre(ix, g.l), cy = cell_centre(iy, g.l), cz = cell_centre(iz, g.l);
+    uint32_t a0 = 0;
+    do {
       const uint32_t na = min((uint32_t)kSfAtomTile, cnt - a0);
       __syncthreads();
       if (threadIdx.x < na) s_at[threadIdx.x] = pk[start + a0 + threadIdx.x];
       __syncthreads();
-      float fr[kSfNodesPerThread], fi[kSfNodesPerThread];
+      float fr[NPT], fi[NPT];
 #pragma unroll
-      for (int u = 0; u < kSfNodesPerThread; u++) { fr[u] = 0.f; fi[u] = 0.f; }
+      for (int i = 0; i < NPT; i++) { fr[i] = 0.f; fi[i] = 0.f; }
+#pragma unroll 1
       for (uint32_t j = 0; j < na; j++) {
         const float4 p = s_at[j];
+        const float uu = fmaf(sx, p.x, fmaf(sy, p.y, sz * p.z));
+        const float nq = -p.w;
 #pragma unroll
-        for (int u = 0; u < kSfNodesPerThread; u++) {
-          const float th = fmaf(kx[u], p.x, fmaf(ky[u], p.y, kz[u] * p.z));
-          float s, c;
-          sfu_sincos(th, &s, &c);
-          fr[u] = fmaf(p.w, c, fr[u]);
-          fi[u] = fmaf(-p.w, s, fi[u]);
+        for (int i = 0; i < NPT - NPOLY; i++) {
+          float sn, cs;
+          sfu_sincos(kap[i] * uu, &sn, &cs);
+          fr[i] = fmaf(p.w, cs, fr[i]);
+          fi[i] = fmaf(nq, sn, fi[i]);
+        }
+#pragma unroll
+        for (int i = NPT - NPOLY; i < NPT; i++) {
+          float sn, cs, qs;
+          fma_sincos_signed(kap[i] * uu, p.w, &sn, &cs, &qs);
+          fr[i] = fmaf(qs, cs, fr[i]);
+          fi[i] = fmaf(-qs, sn, fi[i]);
         }
       }
+      // Tile sums to shared memory in the unit's node order, then one thread
+      // per node (coalesced): FP64 twiddle, S store or add.
+      if (act) {
 #pragma unroll
-      for (int u = 0; u < kSfNodesPerThread; u++) { sr[u] += fr[u]; si[u] += fi[u]; }
-    }
-    const uint32_t ix = cell / (g.ny * g.nz), iy = (cell / g.nz) % g.ny, iz = cell % g.nz;
-    const double cx = cell_centre(ix, g.l), cy = cell_centre(iy, g.l), cz = cell_centre(iz, g.l);
-#pragma unroll
-    for (int u = 0; u < kSfNodesPerThread; u++) {
-      if (!act[u]) continue;
-      const uint32_t k = blockIdx.x * (kSfThreads * kSfNodesPerThread) + u * kSfThreads + threadIdx.x;
-      double ts, tc;
-      sincos(Kx[u] * cx + Ky[u] * cy + Kz[u] * cz, &ts, &tc);
-      // (sr + i si) * (tc - i ts)
-      S[(size_t)cell * ld + k] = make_double2(sr[u] * tc + si[u] * ts, si[u] * tc - sr[u] * ts);
-    }
+        for (int i = 0; i < NPT; i++)
+          if (r0 + i < u.n_rad) s_f[d * u.n_rad + r0 + i] = make_float2(fr[i], fi[i]);
+      }
+      __syncthreads();
+      for (uint32_t m = threadIdx.x; m < nodes; m += kSfThreads) {
+        const uint32_t k = u.node_begin + m;
+        const double4 kn = node64[k];
+        double ts, tc;
+        sincos(kn.x * cx + kn.y * cy + kn.z * cz, &ts, &tc);
+        const float2 f = s_f[m];
+        const double sr = f.x, si = f.y;
+        // (sr + i si) * (tc - i ts)
+        const double2 v = make_double2(sr * tc + si * ts, si * tc - sr * ts);
+        double2 *dst = S + (size_t)cell * ld + k;
+        if (a0 == 0) {
+          *dst = v;
+        } else {
+          const double2 o = *dst;
+          *dst = make_double2(o.x + v.x, o.y + v.y);
+        }
+      }
+      a0 += kSfAtomTile;
+    } while (a0 < cnt);
   }
+}
+
+// node64 and S are offset to the launch's first local node; units index
+// them from there.
+__global__ void __launch_bounds__(kSfThreads, 6)
+k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_count,
+                    const uint32_t *__restrict__ cell_point, Grid g, const SfUnit *__restrict__ units,
+                    const float4 *__restrict__ dirs, const float *__restrict__ kappa,
+                    const double4 *__restrict__ node64, uint32_t ld, double2 *__restrict__ S) {
+  __shared__ float4 s_at[kSfAtomTile];
+  __shared__ float2 s_f[kSfThreads * kSfMaxNpt];
+  const SfUnit u = units[blockIdx.x];
+  const uint32_t c0 = blockIdx.y * kSfCellsPerCta;
+  const uint32_t c1 = min(g.ncell, c0 + kSfCellsPerCta);
+#define GLST_SF_CASE(n) \
+  case n: sf_unit<n>(u, pk, cell_count, cell_point, g, dirs, kappa, node64, ld, c0, c1, S, s_at, s_f); break;
+  switch (u.npt) {
+    GLST_SF_CASE(1) GLST_SF_CASE(2) GLST_SF_CASE(3) GLST_SF_CASE(4) GLST_SF_CASE(5) GLST_SF_CASE(6)
+    GLST_SF_CASE(7) GLST_SF_CASE(8) GLST_SF_CASE(9) GLST_SF_CASE(10) GLST_SF_CASE(11) GLST_SF_CASE(12)
+    default: break;
+  }
+#undef GLST_SF_CASE
 }
 
 // ----------------------------------------------------------------------------
