@@ -223,6 +223,30 @@ __device__ __forceinline__ void fma_sincos_signed(float th, float q, float *s, f
   *qs = __int_as_float(__float_as_int(q) ^ (__float_as_int(t) << 31));
 }
 
+// The same polynomial on two angles at once with the paired FP32
+// instructions of sm_100 (FFMA2/FMUL2/FADD2: two IEEE FP32 operations per
+// instruction, each lane bit-identical to the scalar form above).
+__device__ __forceinline__ float2 bcast(float v) { return make_float2(v, v); }
+
+__device__ __forceinline__ void fma_sincos_signed2(float2 th, float q, float2 *s, float2 *c, float2 *qs) {
+  const float2 t = __ffma2_rn(th, bcast(kInvPi), bcast(kRoundMagic));
+  const float2 n = __fadd2_rn(t, bcast(-kRoundMagic));
+  float2 r = __ffma2_rn(n, bcast(-kPiHi), th);
+  r = __ffma2_rn(n, bcast(-kPiLo), r);
+  const float2 r2 = __fmul2_rn(r, r);
+  float2 p = __ffma2_rn(bcast(kSin4), r2, bcast(kSin3));
+  p = __ffma2_rn(p, r2, bcast(kSin2));
+  p = __ffma2_rn(p, r2, bcast(kSin1));
+  *s = __ffma2_rn(__fmul2_rn(p, r2), r, r);
+  float2 cc = __ffma2_rn(bcast(kCos4), r2, bcast(kCos3));
+  cc = __ffma2_rn(cc, r2, bcast(kCos2));
+  cc = __ffma2_rn(cc, r2, bcast(kCos1));
+  *c = __ffma2_rn(cc, r2, bcast(kCos0));
+  const int qi = __float_as_int(q);
+  *qs = make_float2(__int_as_float(qi ^ (__float_as_int(t.x) << 31)),
+                    __int_as_float(qi ^ (__float_as_int(t.y) << 31)));
+}
+
 // ----------------------------------------------------------------------------
 // Structure factors.  S_c(k) = sum_{j in c} q_j e^{-i k.r_j}
 //                            = e^{-i k.c} sum_j q_j e^{-i k.d_j},  d_j = r_j - c.
@@ -231,9 +255,10 @@ __device__ __forceinline__ void fma_sincos_signed(float th, float q, float *s, f
 // A CTA takes one work unit -- up to 128 / nb directions of one group, nb
 // threads per direction, each thread NPT consecutive radial nodes -- and
 // kSfCellsPerCta consecutive cells.  Per (atom, node): one multiply, a sine
-// and cosine (SFU, or the FMA-pipe polynomial for the last NPOLY slots), two
-// FMAs.  FP32 over a tile of <= kSfAtomTile atoms (|k.d| <~ 25 rad), then
-// FP64: the twiddle e^{-ik.c} and the sum over tiles.
+// and cosine (SFU, or the FMA-pipe polynomial for the last slot pairs), two
+// FMAs, in paired FP32 instructions where two slots go together.  FP32 over a
+// tile of <= kSfAtomTile atoms (|k.d| <~ 25 rad), then FP64: the twiddle
+// e^{-ik.c} and the sum over tiles.
 constexpr int kSfThreads = 128;
 constexpr int kSfMaxNpt = 12;     // radial nodes per thread, at most
 constexpr int kSfCellsPerCta = 2;
@@ -250,9 +275,12 @@ struct SfUnit {
   uint32_t pad;
 };
 
-// FMA-pipe share: about 20 % of the slots (measured on water10k: 1.49 ms
-// with none, 1.34 ms at 20 %, 1.42 ms at 30 %, 1.49 ms at 45 %).
-__host__ __device__ constexpr int sf_poly_slots(int npt) { return (2 * npt + 5) / 10; }
+// Slot pairs on the FMA pipe.  Per slot a polynomial costs ~21 FP32
+// operations and a MUFU slot 4 FP32 operations plus 2 MUFU operations, each of
+// which occupies the SFU for 8 cycles of a warp; the FMA and SFU pipes balance
+// at ~4 polynomial slots of 11.  Measured on water10k: 1.47 ms with none,
+// 1.28 ms with (npt - 1) / 4 pairs, 1.39 ms with (npt + 1) / 4.
+__host__ __device__ constexpr int sf_poly_pairs(int npt) { return (npt - 1) / 4; }
 
 template <int NPT>
 __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restrict__ pk,
@@ -261,7 +289,10 @@ __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restric
                                         const float4 *__restrict__ dirs, const float *__restrict__ kappa,
                                         const double4 *__restrict__ node64, uint32_t ld, uint32_t c0,
                                         uint32_t c1, double2 *__restrict__ S, float4 *s_at, float2 *s_f) {
-  constexpr int NPOLY = sf_poly_slots(NPT);
+  // Slots are handled in pairs (FMUL2/FFMA2); an odd last slot alone.
+  constexpr int NP2 = NPT / 2;
+  constexpr bool ODD = (NPT & 1) != 0;
+  constexpr int POLY2 = sf_poly_pairs(NPT);  // pairs on the FMA pipe (the last ones)
   const uint32_t d = threadIdx.x / u.nb;
   const uint32_t b = threadIdx.x - d * u.nb;
   const bool act = d < u.n_dir;
@@ -274,6 +305,10 @@ __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restric
   float kap[NPT];
 #pragma unroll
   for (int i = 0; i < NPT; i++) kap[i] = (act && r0 + i < u.n_rad) ? kappa[u.kappa_begin + r0 + i] : 0.f;
+  float2 kap2[NP2 > 0 ? NP2 : 1];
+#pragma unroll
+  for (int k = 0; k < NP2; k++) kap2[k] = make_float2(kap[2 * k], kap[2 * k + 1]);
+  const float kap_odd = kap[NPT - 1];
   const uint32_t nodes = u.n_dir * u.n_rad;
   for (uint32_t cell = c0; cell < c1; cell++) {
     const uint32_t cnt = cell_count[cell];
@@ -286,35 +321,50 @@ __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restric
       __syncthreads();
       if (threadIdx.x < na) s_at[threadIdx.x] = pk[start + a0 + threadIdx.x];
       __syncthreads();
-      float fr[NPT], fi[NPT];
+      // FR = sum q cos, FI = sum q sin (the sign of S's imaginary part is
+      // applied when the sums are stored)
+      float2 FR[NP2 > 0 ? NP2 : 1], FI[NP2 > 0 ? NP2 : 1];
 #pragma unroll
-      for (int i = 0; i < NPT; i++) { fr[i] = 0.f; fi[i] = 0.f; }
+      for (int k = 0; k < NP2; k++) { FR[k] = make_float2(0.f, 0.f); FI[k] = make_float2(0.f, 0.f); }
+      float fr_odd = 0.f, fi_odd = 0.f;
 #pragma unroll 1
       for (uint32_t j = 0; j < na; j++) {
         const float4 p = s_at[j];
         const float uu = fmaf(sx, p.x, fmaf(sy, p.y, sz * p.z));
-        const float nq = -p.w;
+        const float2 uu2 = bcast(uu);
+        const float2 q2 = bcast(p.w);
 #pragma unroll
-        for (int i = 0; i < NPT - NPOLY; i++) {
-          float sn, cs;
-          sfu_sincos(kap[i] * uu, &sn, &cs);
-          fr[i] = fmaf(p.w, cs, fr[i]);
-          fi[i] = fmaf(nq, sn, fi[i]);
+        for (int k = 0; k < NP2 - POLY2; k++) {
+          const float2 th = __fmul2_rn(kap2[k], uu2);
+          float sa, ca, sb, cb;
+          sfu_sincos(th.x, &sa, &ca);
+          sfu_sincos(th.y, &sb, &cb);
+          FR[k] = __ffma2_rn(q2, make_float2(ca, cb), FR[k]);
+          FI[k] = __ffma2_rn(q2, make_float2(sa, sb), FI[k]);
         }
 #pragma unroll
-        for (int i = NPT - NPOLY; i < NPT; i++) {
-          float sn, cs, qs;
-          fma_sincos_signed(kap[i] * uu, p.w, &sn, &cs, &qs);
-          fr[i] = fmaf(qs, cs, fr[i]);
-          fi[i] = fmaf(-qs, sn, fi[i]);
+        for (int k = NP2 - POLY2; k < NP2; k++) {
+          float2 sn, cs, qs;
+          fma_sincos_signed2(__fmul2_rn(kap2[k], uu2), p.w, &sn, &cs, &qs);
+          FR[k] = __ffma2_rn(qs, cs, FR[k]);
+          FI[k] = __ffma2_rn(qs, sn, FI[k]);
+        }
+        if (ODD) {
+          float sn, cs;
+          sfu_sincos(kap_odd * uu, &sn, &cs);
+          fr_odd = fmaf(p.w, cs, fr_odd);
+          fi_odd = fmaf(p.w, sn, fi_odd);
         }
       }
       // Tile sums to shared memory in the unit's node order, then one thread
       // per node (coalesced): FP64 twiddle, S store or add.
       if (act) {
 #pragma unroll
-        for (int i = 0; i < NPT; i++)
-          if (r0 + i < u.n_rad) s_f[d * u.n_rad + r0 + i] = make_float2(fr[i], fi[i]);
+        for (int k = 0; k < NP2; k++) {
+          if (r0 + 2 * k < u.n_rad) s_f[d * u.n_rad + r0 + 2 * k] = make_float2(FR[k].x, -FI[k].x);
+          if (r0 + 2 * k + 1 < u.n_rad) s_f[d * u.n_rad + r0 + 2 * k + 1] = make_float2(FR[k].y, -FI[k].y);
+        }
+        if (ODD && r0 + NPT - 1 < u.n_rad) s_f[d * u.n_rad + r0 + NPT - 1] = make_float2(fr_odd, -fi_odd);
       }
       __syncthreads();
       for (uint32_t m = threadIdx.x; m < nodes; m += kSfThreads) {
