@@ -553,14 +553,27 @@ struct LrChunk {
 
 // A CTA takes 128 consecutive cell-ordered atoms whatever their cells (so
 // every warp is full -- one CTA per cell left ~10-15 % of the lanes of last
-// warps idle, measured 2.06 vs 1.63 ms on water10k), and stages
-// the R' tiles of the up to kLrfCells cells those atoms belong to; lanes read
-// their own cell's tile (at most a few distinct addresses per warp).  Atoms
-// of sparser ranges (more cells) are handled in several passes over windows
-// of kLrfCells cells.  Per (atom, node) pair: the arithmetic above.
-constexpr int kLrfCells = 4;          // cells staged per pass
-constexpr int kLrfTileNodes = 256;    // nodes per cell tile
-constexpr int kLrfPerThread = (kLrfCells * kLrfTileNodes) / kLrThreads;
+// warps idle, measured 2.06 vs 1.63 ms on water10k), and stages the R' tiles
+// of the up to kLrfCells cells those atoms belong to; lanes read their own
+// cell's tile.  Atoms of sparser ranges (more cells) are handled in several
+// passes over windows of kLrfCells cells.
+//
+// Radial nodes go in pairs (r, r+1) -- a direction with an odd count gets a
+// zero node -- stored as float4 (R'x_r, R'x_r+1, R'y_r, R'y_r+1) so that the
+// paired FP32 instructions (FMUL2/FFMA2) do two nodes at once:
+//   EA += c R'x,  EB += s R'y,  G += kappa (c R'y + s R'x),   e = EA - EB.
+// All sines and cosines come from the SFU: moving 20-40 % of the pairs to
+// the FMA-pipe polynomial measured slower here (1.63-1.87 ms vs 1.56 ms on
+// water10k), the FMA pipe already carrying ~7 FP32 operations per node.
+// The cell slots of a tile are kLrfSlotPad float4 apart beyond the tile so
+// that the up to four addresses a warp reads fall in different shared-memory
+// banks (32.9 M bank conflicts per launch without the pad, 0.25 M with).
+constexpr int kLrfCells = 4;           // cells staged per pass
+constexpr int kLrfTilePairs = 128;     // node pairs per cell tile
+constexpr int kLrfTileNodes = 2 * kLrfTilePairs;
+constexpr int kLrfSlotPad = 2;
+constexpr int kLrfSlot = kLrfTilePairs + kLrfSlotPad;
+constexpr int kLrfPerThread = (kLrfCells * kLrfTilePairs) / kLrThreads;
 
 __device__ __forceinline__ uint32_t cell_of_atom(const uint32_t *__restrict__ cell_point, uint32_t ncell,
                                                  uint32_t p) {
@@ -574,22 +587,26 @@ __device__ __forceinline__ uint32_t cell_of_atom(const uint32_t *__restrict__ ce
   return lo;
 }
 
-__global__ void __launch_bounds__(kLrThreads, 8)
+__global__ void __launch_bounds__(kLrThreads, 6)
 k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_point, uint32_t ncell,
                   const LrChunk *__restrict__ chunks, const float4 *__restrict__ dirs,
                   const float *__restrict__ kappa, const float2 *__restrict__ R, uint32_t K, uint32_t natom,
                   double4 *__restrict__ part) {
-  __shared__ float4 s_n[2][kLrfCells * kLrfTileNodes];  // per cell slot: (R'x, R'y, kappa_r, 0)
-  __shared__ float s_kappa[kLrfTileNodes];
+  __shared__ float4 s_n[2][kLrfCells * kLrfSlot];
+  __shared__ float2 s_kappa2[kLrfTilePairs];
   __shared__ uint32_t s_range[2];
   const uint32_t a0 = blockIdx.x * kLrThreads;
   const uint32_t p = a0 + threadIdx.x;
   const bool active = p < natom;
   const LrChunk ch = chunks[blockIdx.y];
   const uint32_t nr = ch.n_rad;
-  const uint32_t dirs_per_tile = max(1u, kLrfTileNodes / nr);  // nr <= kLrfTileNodes (host check)
+  const uint32_t npr = (nr + 1) >> 1;                                   // pairs per direction
+  const uint32_t dirs_per_tile = max(1u, (uint32_t)kLrfTilePairs / npr);  // npr <= kLrfTilePairs (host check)
   const uint32_t ntiles = (ch.n_dir + dirs_per_tile - 1) / dirs_per_tile;
-  for (uint32_t t = threadIdx.x; t < nr; t += kLrThreads) s_kappa[t] = kappa[ch.kappa_begin + t];
+  for (uint32_t t = threadIdx.x; t < npr; t += kLrThreads) {
+    const uint32_t r = 2 * t;
+    s_kappa2[t] = make_float2(kappa[ch.kappa_begin + r], r + 1 < nr ? kappa[ch.kappa_begin + r + 1] : 0.f);
+  }
   const uint32_t last = min(a0 + kLrThreads, natom) - 1;
   if (threadIdx.x == 0) s_range[0] = cell_of_atom(cell_point, ncell, a0);
   if (threadIdx.x == 1) s_range[1] = cell_of_atom(cell_point, ncell, last);
@@ -603,20 +620,26 @@ k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ ce
     const bool mine = active && my_cell >= w0 && my_cell < w0 + nc;
     const uint32_t slot = mine ? my_cell - w0 : 0;
     const bool warp_live = __any_sync(0xffffffffu, mine);
-    float2 pre[kLrfPerThread];
-    // prefetch tile 0 of every cell of this window
+    float4 pre[kLrfPerThread];
+    // prefetch one tile of every cell of this window into registers
     auto prefetch = [&](uint32_t d0) {
       const uint32_t nd = min(dirs_per_tile, ch.n_dir - d0);
 #pragma unroll
       for (int k = 0; k < kLrfPerThread; k++) {
         const uint32_t t = threadIdx.x + k * kLrThreads;
-        const uint32_t c = t / kLrfTileNodes, i = t % kLrfTileNodes;
-        pre[k] = (c < nc && i < nd * nr)
-                     ? R[(size_t)(w0 + c) * K + ch.node_begin + (size_t)d0 * nr + i]
-                     : make_float2(0.f, 0.f);
+        const uint32_t c = t / kLrfTilePairs, i = t % kLrfTilePairs;
+        const uint32_t dd = i / npr, r = 2 * (i - dd * npr);
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (c < nc && dd < nd) {
+          const float2 *src = R + (size_t)(w0 + c) * K + ch.node_begin + (size_t)(d0 + dd) * nr + r;
+          const float2 x0 = src[0];
+          const float2 x1 = (r + 1 < nr) ? src[1] : make_float2(0.f, 0.f);
+          v = make_float4(x0.x, x1.x, x0.y, x1.y);
+        }
+        pre[k] = v;
       }
     };
-    __syncthreads();  // previous window done with s_n; s_kappa visible after the next barrier
+    __syncthreads();  // previous window done with s_n
     prefetch(0);
     for (uint32_t tile = 0; tile < ntiles; tile++) {
       const uint32_t d0 = tile * dirs_per_tile;
@@ -625,42 +648,34 @@ k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ ce
 #pragma unroll
       for (int k = 0; k < kLrfPerThread; k++) {
         const uint32_t t = threadIdx.x + k * kLrThreads;
-        const uint32_t i = t % kLrfTileNodes;
-        if (t / kLrfTileNodes < nc && i < nd * nr) buf[t] = make_float4(pre[k].x, pre[k].y, s_kappa[i % nr], 0.f);
+        buf[(t / kLrfTilePairs) * kLrfSlot + t % kLrfTilePairs] = pre[k];
       }
       __syncthreads();
       if (tile + 1 < ntiles) prefetch(d0 + dirs_per_tile);
       if (warp_live) {
         float tx = 0.f, ty = 0.f, tz = 0.f, te = 0.f;
-        const float4 *cb = buf + slot * kLrfTileNodes;
+        const float4 *cb = buf + slot * kLrfSlot;
         for (uint32_t d = 0; d < nd; d++) {
           const float4 sj = dirs[ch.dir_begin + d0 + d];
           const float u = fmaf(sj.x, pa.x, fmaf(sj.y, pa.y, sj.z * pa.z));
-          float ea = 0.f, eb = 0.f, ec = 0.f, ed = 0.f, ga = 0.f, gb = 0.f;
-          const float4 *nn = cb + d * nr;
-          uint32_t r = 0;
+          const float2 u2 = bcast(u);
+          float2 EA = make_float2(0.f, 0.f), EB = make_float2(0.f, 0.f), G = make_float2(0.f, 0.f);
+          const float4 *nn = cb + d * npr;
 #pragma unroll 2
-          for (; r + 1 < nr; r += 2) {
-            const float4 v0 = nn[r], v1 = nn[r + 1];
+          for (uint32_t k = 0; k < npr; k++) {
+            const float4 v = nn[k];
+            const float2 kp = s_kappa2[k];
+            const float2 th = __fmul2_rn(kp, u2);
             float s0, c0, s1, c1;
-            sfu_sincos(v0.z * u, &s0, &c0);
-            sfu_sincos(v1.z * u, &s1, &c1);
-            ea = fmaf(c0, v0.x, ea);
-            eb = fmaf(-s0, v0.y, eb);
-            ec = fmaf(c1, v1.x, ec);
-            ed = fmaf(-s1, v1.y, ed);
-            ga = fmaf(v0.z, fmaf(c0, v0.y, s0 * v0.x), ga);
-            gb = fmaf(v1.z, fmaf(c1, v1.y, s1 * v1.x), gb);
+            sfu_sincos(th.x, &s0, &c0);
+            sfu_sincos(th.y, &s1, &c1);
+            const float2 C = make_float2(c0, c1), Sn = make_float2(s0, s1);
+            const float2 RX = make_float2(v.x, v.y), RY = make_float2(v.z, v.w);
+            EA = __ffma2_rn(C, RX, EA);
+            EB = __ffma2_rn(Sn, RY, EB);
+            G = __ffma2_rn(kp, __ffma2_rn(C, RY, __fmul2_rn(Sn, RX)), G);
           }
-          if (r < nr) {
-            const float4 v0 = nn[r];
-            float s0, c0;
-            sfu_sincos(v0.z * u, &s0, &c0);
-            ea = fmaf(c0, v0.x, ea);
-            eb = fmaf(-s0, v0.y, eb);
-            ga = fmaf(v0.z, fmaf(c0, v0.y, s0 * v0.x), ga);
-          }
-          const float e = (ea + eb) + (ec + ed), gsum = ga + gb;
+          const float e = (EA.x + EA.y) - (EB.x + EB.y), gsum = G.x + G.y;
           te += e;
           tx = fmaf(gsum, sj.x, tx);
           ty = fmaf(gsum, sj.y, ty);
