@@ -121,7 +121,7 @@ struct glst_handle {
   int nsm = 148;
   std::vector<uint32_t> g_node_base, g_dir_base, g_kappa_base;  // per group, internal order
   uint32_t sat_nb = 1, sat_stride = 0;
-  size_t sat_smem = 0;
+  bool sat_xyz = true;  // shell-sum cell-coordinate table in shared memory
   uint32_t combine_blocks = 1;
   bool computed = false;
   std::vector<DevBuf> bufs;
@@ -244,6 +244,12 @@ static Tuning tuned(const Plan &p, uint32_t K) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
   auto it = g_tune.find(tune_key(p, K));
   return it == g_tune.end() ? Tuning{} : it->second;
+}
+
+static uint32_t pow2_floor(uint32_t v) {
+  uint32_t p = 1;
+  while (p * 2 <= v && p < 32) p *= 2;
+  return p;
 }
 
 static constexpr uint32_t kFarStages = 1;  // far-field pipeline stages per solve (see below)
@@ -475,28 +481,30 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
     h->sat_stride = (uint32_t)(C + 1);
     while (h->sat_stride % 8 != 1) h->sat_stride++;
     const size_t per_node = ((size_t)h->sat_stride + p.n[0] + p.n[1] + p.n[2]) * sizeof(double2);
-    const size_t budget = std::min<size_t>((size_t)smem_optin, 200 * 1024);
-    if (per_node > budget)
+    // the cell-coordinate table (4 bytes per cell) comes off the budget when
+    // a row and the table fit together; otherwise the kernel divides
+    const size_t smem_total = (size_t)smem_optin;
+    const size_t xyz_bytes = (C * 4 + 15) & ~size_t(15);
+    h->sat_xyz = per_node + xyz_bytes <= smem_total;
+    const size_t budget = h->sat_xyz ? smem_total - xyz_bytes : smem_total;
+    if (p.n[0] >= 1024 || p.n[1] >= 1024 || p.n[2] >= 1024 || per_node > budget)
       return fail(GLST_ERR_SIZE,
                   "cell grid of %zu cells exceeds the shell-sum shared-memory limit (%zu cells)",
                   C, budget / sizeof(double2) - 1);
     h->sat_per_node = per_node;
     h->sat_budget = budget;
-    h->sat_nb = (uint32_t)std::max<size_t>(1, std::min<size_t>(16, (100 * 1024) / per_node));
-    h->sat_smem = per_node * h->sat_nb;
+    h->sat_nb = pow2_floor((uint32_t)std::max<size_t>(1, std::min<size_t>(8, budget / per_node)));
     // one process-wide maximum, so handles with different plans coexist
     CUDA_TRY(cudaFuncSetAttribute(dev::k_shell_sums, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)budget));
+                                  (int)smem_total));
     h->nsm = nsm;
     h->g_node_base = node_base;
     h->g_dir_base = dir_base;
     h->g_kappa_base = kappa_base;
     {
       const Tuning t = tuned(p, h->K);
-      if (t.sat_nb) {
-        h->sat_nb = std::min<uint32_t>(t.sat_nb, (uint32_t)std::max<size_t>(1, budget / per_node));
-        h->sat_smem = per_node * h->sat_nb;
-      }
+      if (t.sat_nb)
+        h->sat_nb = pow2_floor(std::min<uint32_t>(t.sat_nb, (uint32_t)std::max<size_t>(1, budget / per_node)));
       if (t.lr_waves) h->lr_waves = t.lr_waves;
     }
     GLST_TRY(build_chunks(h));
@@ -567,10 +575,13 @@ static glst_status sf_range(glst_handle *h, uint32_t u0, uint32_t u1, cudaStream
 
 static glst_status shell_range(glst_handle *h, uint32_t kb, uint32_t ke, cudaStream_t st) {
   if (ke <= kb || !h->plan.natom) return GLST_OK;
+  uint32_t lg = 0;
+  while ((1u << lg) < h->sat_nb) lg++;
   dev::SatArgs a{h->S + kb, h->node64 + h->k_begin + kb, h->node_radii + h->k_begin + kb, ke - kb, h->K,
-                 h->sat_nb, h->sat_stride, h->R + kb};
+                 h->sat_nb, lg, h->sat_xyz ? 1u : 0u, h->sat_stride, h->R + kb};
   const uint32_t nblk = (ke - kb + h->sat_nb - 1) / h->sat_nb;
-  dev::k_shell_sums<<<nblk, dev::kSatThreads, h->sat_smem, st>>>(h->grid, a);
+  const size_t smem = h->sat_per_node * h->sat_nb + (h->sat_xyz ? (((size_t)h->plan.ncell * 4 + 15) & ~size_t(15)) : 0);
+  dev::k_shell_sums<<<nblk, dev::kSatThreads, smem, st>>>(h->grid, a);
   CUDA_TRY(cudaGetLastError());
   return GLST_OK;
 }
@@ -958,13 +969,11 @@ glst_status glst_autotune(glst_handle *h, const double *rx, const double *ry, co
     for (uint32_t nb : {1u, 2u, 4u, 8u, 16u, 32u}) {
       if (h->sat_per_node * nb > h->sat_budget) break;
       h->sat_nb = nb;
-      h->sat_smem = h->sat_per_node * nb;
       float ms = 0.f;
       GLST_TRY(timed(phase_shell, &ms));
       if (ms < best) best = ms, best_nb = nb;
     }
     h->sat_nb = best_nb;
-    h->sat_smem = h->sat_per_node * best_nb;
     GLST_TRY(phase_shell(h, st));
     // long-range gather: waves of chunk CTAs
     uint32_t best_w = h->lr_waves;

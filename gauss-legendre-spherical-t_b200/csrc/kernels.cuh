@@ -426,8 +426,10 @@ struct SatArgs {
   const uint32_t *node_radii;   // r_in | r_out << 16
   uint32_t K;                   // nodes handled by this launch
   uint32_t ld;                  // row stride of S and R (nodes per cell row)
-  uint32_t nb;                  // nodes per CTA
-  uint32_t stride;              // shared row stride (complex) = ncell + 1
+  uint32_t nb;                  // nodes per CTA (a power of two, <= 32)
+  uint32_t lg_nb;               // log2(nb)
+  uint32_t xyz_table;           // 1: cell coordinates tabulated in shared memory
+  uint32_t stride;              // shared row stride (complex), >= ncell, = 1 (mod 8)
   float2 *R;
 };
 
@@ -458,20 +460,33 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// Dynamic shared memory: nb rows of `stride` complex (the SAT), then the
-// twiddle tables nb x (nx + ny + nz) complex.
+// Dynamic shared memory: nb rows of `stride` complex (the SAT), the twiddle
+// tables nb x (nx + ny + nz) complex, then (when it fits) the cell coordinates
+// (ncell x u32, x | y << 10 | z << 20).  nb is a power of two <= 32: lane l of a warp works
+// on node l % nb of the CTA and on the (l / nb)-th of the 32 / nb cells or
+// lines the warp takes per step, so the per-node values (radii, weight,
+// twiddle rows) stay in registers and the S loads and R stores of a warp are
+// runs of consecutive nodes.
 __global__ void __launch_bounds__(kSatThreads)
 k_shell_sums(Grid g, SatArgs a) {
   extern __shared__ double2 s_sat[];
-  const uint32_t k0 = blockIdx.x * a.nb;
-  const uint32_t nb = min(a.nb, a.K - k0);
+  const uint32_t nb = a.nb, lg = a.lg_nb;
+  const uint32_t k0 = blockIdx.x * nb;
   const uint32_t C = g.ncell;
   const uint32_t naxis = g.nx + g.ny + g.nz;
-  double2 *s_tw = s_sat + (size_t)a.nb * a.stride;
+  double2 *s_tw = s_sat + (size_t)nb * a.stride;
+  uint32_t *s_xyz = reinterpret_cast<uint32_t *>(s_tw + (size_t)nb * naxis);
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t j = lane & (nb - 1u);
+  const uint32_t per_warp = 32u >> lg;
+  const uint32_t first = warp * per_warp + (lane >> lg);
+  const uint32_t step = (blockDim.x >> 5) * per_warp;
+  const uint32_t k = k0 + j;
+  const bool jv = k < a.K;
   // twiddle tables: e^{i k_a (i + 1/2) l} per node and axis
   for (uint32_t t = threadIdx.x; t < nb * naxis; t += blockDim.x) {
-    const uint32_t j = t / naxis, r = t % naxis;
-    const double4 nk = a.node64[k0 + j];
+    const uint32_t jj = t / naxis, r = t - jj * naxis;
+    const double4 nk = (k0 + jj < a.K) ? a.node64[k0 + jj] : make_double4(0.0, 0.0, 0.0, 0.0);
     double kc;
     if (r < g.nx) kc = nk.x * cell_centre(r, g.l);
     else if (r < g.nx + g.ny) kc = nk.y * cell_centre(r - g.nx, g.l);
@@ -480,54 +495,56 @@ k_shell_sums(Grid g, SatArgs a) {
     sincos(kc, &sn, &cs);
     s_tw[t] = make_double2(cs, sn);
   }
-  // load S[c][k0 .. k0+nb) -> s_sat[j*stride + c]
-#pragma unroll 4
-  for (uint32_t t = threadIdx.x; t < C * nb; t += blockDim.x) {
-    const uint32_t c = t / nb, j = t % nb;
-    s_sat[j * a.stride + c] = a.S[(size_t)c * a.ld + k0 + j];
+  auto coords = [&](uint32_t c) {
+    const uint32_t x = c / (g.ny * g.nz), rem = c - x * (g.ny * g.nz);
+    const uint32_t y = rem / g.nz, z = rem - y * g.nz;
+    return x | (y << 10) | (z << 20);
+  };
+  if (a.xyz_table)
+    for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) s_xyz[c] = coords(c);
+  double2 *row = s_sat + (size_t)j * a.stride;
+  // S[c][k0 + j] -> row j
+  for (uint32_t c = first; c < C; c += step)
+    row[c] = jv ? a.S[(size_t)c * a.ld + k] : make_double2(0.0, 0.0);
+  __syncthreads();
+  // prefix along z (lines x, y)
+  for (uint32_t l = first; l < g.nx * g.ny; l += step) {
+    double2 *p = row + l * g.nz;
+    double2 acc = make_double2(0.0, 0.0);
+    for (uint32_t z = 0; z < g.nz; z++) { acc.x += p[z].x; acc.y += p[z].y; p[z] = acc; }
   }
   __syncthreads();
-  // prefix along z (lines indexed by node, x, y)
-  for (uint32_t t = threadIdx.x; t < nb * g.nx * g.ny; t += blockDim.x) {
-    const uint32_t j = t / (g.nx * g.ny), xy = t % (g.nx * g.ny);
-    double2 *row = s_sat + j * a.stride + xy * g.nz;
+  // prefix along y (lines x, z)
+  for (uint32_t l = first; l < g.nx * g.nz; l += step) {
+    const uint32_t x = l / g.nz, z = l - x * g.nz;
+    double2 *p = row + x * g.ny * g.nz + z;
     double2 acc = make_double2(0.0, 0.0);
-    for (uint32_t z = 0; z < g.nz; z++) { acc.x += row[z].x; acc.y += row[z].y; row[z] = acc; }
+    for (uint32_t y = 0; y < g.ny; y++) { acc.x += p[y * g.nz].x; acc.y += p[y * g.nz].y; p[y * g.nz] = acc; }
   }
   __syncthreads();
-  // prefix along y (lines indexed by node, x, z)
-  for (uint32_t t = threadIdx.x; t < nb * g.nx * g.nz; t += blockDim.x) {
-    const uint32_t j = t / (g.nx * g.nz), xz = t % (g.nx * g.nz);
-    const uint32_t x = xz / g.nz, z = xz % g.nz;
-    double2 *row = s_sat + j * a.stride;
-    double2 acc = make_double2(0.0, 0.0);
-    for (uint32_t y = 0; y < g.ny; y++) {
-      double2 &v = row[(x * g.ny + y) * g.nz + z];
-      acc.x += v.x; acc.y += v.y; v = acc;
+  // prefix along x (lines y, z)
+  {
+    const uint32_t sx = g.ny * g.nz;
+    for (uint32_t l = first; l < sx; l += step) {
+      double2 *p = row + l;
+      double2 acc = make_double2(0.0, 0.0);
+      for (uint32_t x = 0; x < g.nx; x++) { acc.x += p[x * sx].x; acc.y += p[x * sx].y; p[x * sx] = acc; }
     }
   }
   __syncthreads();
-  // prefix along x (lines indexed by node, y, z)
-  for (uint32_t t = threadIdx.x; t < nb * g.ny * g.nz; t += blockDim.x) {
-    const uint32_t j = t / (g.ny * g.nz), yz = t % (g.ny * g.nz);
-    double2 *row = s_sat + j * a.stride + yz;
-    double2 acc = make_double2(0.0, 0.0);
-    const uint32_t step = g.ny * g.nz;
-    for (uint32_t x = 0; x < g.nx; x++) { acc.x += row[x * step].x; acc.y += row[x * step].y; row[x * step] = acc; }
-  }
-  __syncthreads();
-  // shell sums, weight and twiddle; consecutive threads -> consecutive nodes
-  for (uint32_t t = threadIdx.x; t < C * nb; t += blockDim.x) {
-    const uint32_t c = t / nb, j = t % nb, k = k0 + j;
-    const uint32_t x = c / (g.ny * g.nz), y = (c / g.nz) % g.ny, z = c % g.nz;
-    const uint32_t radii = a.node_radii[k];
-    const double2 *row = s_sat + j * a.stride;
-    const double2 o = cube_sum(row, x, y, z, radii >> 16, g);
-    const double2 i = cube_sum(row, x, y, z, radii & 0xffffu, g);
-    const double w = a.node64[k].w;
+  if (!jv) return;
+  // shell sums, weight and twiddle
+  const uint32_t radii = a.node_radii[k];
+  const uint32_t r_out = radii >> 16, r_in = radii & 0xffffu;
+  const double w = a.node64[k].w;
+  const double2 *twx = s_tw + (size_t)j * naxis, *twy = twx + g.nx, *twz = twy + g.ny;
+  for (uint32_t c = first; c < C; c += step) {
+    const uint32_t xyz = a.xyz_table ? s_xyz[c] : coords(c);
+    const uint32_t x = xyz & 1023u, y = (xyz >> 10) & 1023u, z = xyz >> 20;
+    const double2 o = cube_sum(row, x, y, z, r_out, g);
+    const double2 i = cube_sum(row, x, y, z, r_in, g);
     const double2 sh = make_double2((o.x - i.x) * w, (o.y - i.y) * w);
-    const double2 *tw = s_tw + j * naxis;
-    const double2 r = cmul(cmul(sh, tw[x]), cmul(tw[g.nx + y], tw[g.nx + g.ny + z]));
+    const double2 r = cmul(cmul(sh, twx[x]), cmul(twy[y], twz[z]));
     a.R[(size_t)c * a.ld + k] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
   }
 }
