@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--reference-log", default=None, metavar="PATH",
+                    help="also write the flagship run as a log in the reference driver's layout "
+                         "(test/full_example.cu), which utils/parse_glst_results.py reads")
     return ap.parse_args()
 
 
@@ -271,6 +274,43 @@ def run_serve(g, n_requests=120, loads=(0.5, 0.8, 1.1), budget=150 << 30, nslots
     return out
 
 
+def write_reference_log(path, workload, g, f, inf, sysd, d, stream, dev, torch, iters=20):
+    """The flagship system as the reference's driver reports it: per-phase
+    times over `iters` solves (phases one after another, each bracketed by
+    CUDA events), direct Coulomb on the GPU, error report vs Coulomb."""
+    from glst_b200 import reports
+    names = ["assign", "near_field", "structure_factors", "shell_sums", "long_range", "combine"]
+    calls = [lambda: f.assign_atoms(*d, stream=stream), lambda: f.calc_sr_ef(stream=stream),
+             lambda: f.calc_sf(stream=stream), lambda: f.sum_rmt_sf(stream=stream),
+             lambda: f.calc_lr_ef(stream=stream), lambda: f.comm_ef(stream=stream)]
+    per = {k: [] for k in names}
+    for _ in range(iters):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(calls) + 1)]
+        ev[0].record(stream)
+        for i, c in enumerate(calls):
+            c()
+            ev[i + 1].record(stream)
+        torch.cuda.synchronize()
+        for i, k in enumerate(names):
+            per[k].append(ev[i].elapsed_time(ev[i + 1]))
+    glst = f.get_ef()
+    n = len(sysd["x"])
+    co = [torch.empty(n, dtype=torch.float64, device=dev) for _ in range(4)]
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record(stream)
+    g.direct_coulomb(*d, *co, stream=stream)
+    c1.record(stream)
+    torch.cuda.synchronize()
+    coul = [t.cpu().numpy() for t in co]
+    L = sysd["box"]
+    meta = {"sweep": "bench", "sys": workload, "tol": "%g" % sysd["tol"],
+            "box_dim": "%g,%g,%g" % tuple(L), "cut": "%g" % sysd["rcut"], "requested_gpus": "1"}
+    text = reports.format_run_log(meta, inf, L, per, c0.elapsed_time(c1), reports.error_stats(glst, coul),
+                                  sysd["tol"])
+    with open(path, "w") as fh:
+        fh.write(text)
+
+
 def run_ours(args, world, rank, local, dist):
     import torch
     g = __graft_entry__.load_package()
@@ -393,6 +433,8 @@ def run_ours(args, world, rank, local, dist):
         "roofline": roofline,
         "wall_s_timed": wall,
     }
+    if rank == 0 and args.reference_log:
+        write_reference_log(args.reference_log, args.workload, g, f, inf, sysd, d, stream, dev, torch, iters=20)
     if world == 1 and not args.no_batch:
         line["batched_vs_plain"] = run_batch(g, torch, dev, stream, n_steps=max(2, args.steps // 5))
     if world == 1 and not args.no_serve:

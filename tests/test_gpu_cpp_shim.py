@@ -17,8 +17,10 @@ def test_cpp_client_runs(tmp_path, pkg):
     if not (shutil.which("nvcc") or os.path.exists("/usr/local/cuda/bin/nvcc")):
         pytest.skip("nvcc not available")
     exe = build_client(str(tmp_path))
-    out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split()
-    e_sum, e_dev, fx0 = (float(v) for v in out)
+    stdout = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+    # the set-up summary the reference prints from init comes first
+    assert "Total number of cubature nodes:" in stdout
+    e_sum, e_dev, fx0 = (float(v) for v in stdout.split()[-3:])
     x = [1, 2, 3, 11, 12, 13]
     y = [1, 2, 1, 12, 11, 12]
     z = [1, 1, 2, 13, 12, 11]
