@@ -579,9 +579,12 @@ struct LrChunk {
 // zero node -- stored as float4 (R'x_r, R'x_r+1, R'y_r, R'y_r+1) so that the
 // paired FP32 instructions (FMUL2/FFMA2) do two nodes at once:
 //   EA += c R'x,  EB += s R'y,  G += kappa (c R'y + s R'x),   e = EA - EB.
-// All sines and cosines come from the SFU: moving 20-40 % of the pairs to
-// the FMA-pipe polynomial measured slower here (1.63-1.87 ms vs 1.56 ms on
-// water10k), the FMA pipe already carrying ~7 FP32 operations per node.
+// One pair in kLrGroup takes its sine and cosine from the FMA-pipe
+// polynomial, interleaved with the SFU pairs of its group (the FMA pipe
+// already carries ~7 FP32 operations per node, so only a small share pays):
+// water10k 1.57 ms with none, 1.51 ms with 1 in 7, 1.53 with 1 in 5, 1.66
+// with 1 in 3; a separate polynomial loop after the SFU loop (20-40 %)
+// measured 1.63-1.87 ms.
 // The cell slots of a tile are kLrfSlotPad float4 apart beyond the tile so
 // that the up to four addresses a warp reads fall in different shared-memory
 // banks (32.9 M bank conflicts per launch without the pad, 0.25 M with).
@@ -591,6 +594,7 @@ constexpr int kLrfTileNodes = 2 * kLrfTilePairs;
 constexpr int kLrfSlotPad = 2;
 constexpr int kLrfSlot = kLrfTilePairs + kLrfSlotPad;
 constexpr int kLrfPerThread = (kLrfCells * kLrfTilePairs) / kLrThreads;
+constexpr int kLrGroup = 7;  // node pairs per group, the last one on the FMA pipe
 
 __device__ __forceinline__ uint32_t cell_of_atom(const uint32_t *__restrict__ cell_point, uint32_t ncell,
                                                  uint32_t p) {
@@ -678,8 +682,35 @@ k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ ce
           const float2 u2 = bcast(u);
           float2 EA = make_float2(0.f, 0.f), EB = make_float2(0.f, 0.f), G = make_float2(0.f, 0.f);
           const float4 *nn = cb + d * npr;
-#pragma unroll 2
-          for (uint32_t k = 0; k < npr; k++) {
+          // groups of kLrGroup pairs: the last of each group takes its sine
+          // and cosine from the FMA-pipe polynomial, interleaved with the SFU
+          // pairs of the same group; the remaining pairs use the SFU
+          uint32_t k = 0;
+          for (; k + kLrGroup <= npr; k += kLrGroup) {
+#pragma unroll
+            for (int q = 0; q < kLrGroup; q++) {
+              const float4 v = nn[k + q];
+              const float2 kp = s_kappa2[k + q];
+              const float2 th = __fmul2_rn(kp, u2);
+              float2 C, Sn, RX = make_float2(v.x, v.y), RY = make_float2(v.z, v.w);
+              if (q == kLrGroup - 1) {
+                float2 sg;
+                fma_sincos_signed2(th, 1.0f, &Sn, &C, &sg);  // sg = (+-1, +-1)
+                RX = __fmul2_rn(RX, sg);
+                RY = __fmul2_rn(RY, sg);
+              } else {
+                float s0, c0, s1, c1;
+                sfu_sincos(th.x, &s0, &c0);
+                sfu_sincos(th.y, &s1, &c1);
+                C = make_float2(c0, c1);
+                Sn = make_float2(s0, s1);
+              }
+              EA = __ffma2_rn(C, RX, EA);
+              EB = __ffma2_rn(Sn, RY, EB);
+              G = __ffma2_rn(kp, __ffma2_rn(C, RY, __fmul2_rn(Sn, RX)), G);
+            }
+          }
+          for (; k < npr; k++) {
             const float4 v = nn[k];
             const float2 kp = s_kappa2[k];
             const float2 th = __fmul2_rn(kp, u2);
