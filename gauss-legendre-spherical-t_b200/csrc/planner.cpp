@@ -306,6 +306,46 @@ static unsigned select_tdesign(const std::vector<double> *&design,
   return t_last;
 }
 
+// The rules of a group depend only on (tol, rmax, alpha, zcut) and the store:
+// cells of the same edge give the same first groups on every grid, so the
+// (costly) selection is kept per parameter set.  Same arithmetic either way.
+struct RuleKey {
+  double tol, dist, alpha, zcut;
+  const TDesignStore *store;
+  bool operator<(const RuleKey &o) const {
+    return std::tie(tol, dist, alpha, zcut, store) < std::tie(o.tol, o.dist, o.alpha, o.zcut, o.store);
+  }
+};
+struct Rules {
+  unsigned gl_degree = 0, t_degree = 0;
+  std::vector<double> xs, ws;
+  const std::vector<double> *design = nullptr;
+};
+static std::mutex g_rule_mu;
+static std::map<RuleKey, Rules> g_rule_cache;
+
+static void select_rules(GroupPlan &g, std::vector<double> &xs, std::vector<double> &ws,
+                         const std::vector<double> *&design, TDesignStore &store, double tol) {
+  const RuleKey key{tol, g.rmax, g.alpha, g.zcut, &store};
+  {
+    std::lock_guard<std::mutex> lk(g_rule_mu);
+    auto it = g_rule_cache.find(key);
+    if (it != g_rule_cache.end()) {
+      g.gl_degree = it->second.gl_degree;
+      g.t_degree = it->second.t_degree;
+      xs = it->second.xs;
+      ws = it->second.ws;
+      design = it->second.design;
+      return;
+    }
+  }
+  g.gl_degree = select_gl(xs, ws, tol, g.rmax, g.alpha, g.zcut);
+  g.t_degree = select_tdesign(design, store, g.gl_degree, xs, ws, tol, g.rmax, g.alpha, g.zcut);
+  std::lock_guard<std::mutex> lk(g_rule_mu);
+  if (g_rule_cache.size() > 1024) g_rule_cache.clear();
+  g_rule_cache[key] = Rules{g.gl_degree, g.t_degree, xs, ws, design};
+}
+
 struct PlanKey {
   double tol;
   int ct_float;
@@ -421,10 +461,8 @@ Plan make_plan(uint32_t natom, double tol, const double box[3], double rcut,
   for (size_t gi = 0; gi < p.groups.size(); gi++) {
     GroupPlan &g = p.groups[gi];
     std::vector<double> xs, ws;
-    g.gl_degree = select_gl(xs, ws, tol, g.rmax, g.alpha, g.zcut);
     const std::vector<double> *sm = nullptr;
-    g.t_degree = select_tdesign(sm, store, g.gl_degree, xs, ws, tol, g.rmax,
-                                g.alpha, g.zcut);
+    select_rules(g, xs, ws, sm, store, tol);
     const size_t m = sm->size() / 3;
     g.n_radial = static_cast<unsigned>(xs.size());
     g.n_dir = static_cast<unsigned>(m);
