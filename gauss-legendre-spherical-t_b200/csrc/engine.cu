@@ -1278,12 +1278,12 @@ glst_status glst_batch_system(glst_batch *b, uint32_t i, glst_handle **h) {
 
 // ---------------------------------------------------------------- request server
 //
-// Continuous batching of independent energy+force requests.  Two threads:
+// Continuous batching of independent energy+force requests.  Threads:
 //   worker  -- completes finished requests, admits queued ones (reserving
 //              device memory against the budget, evicting idle resident
 //              systems least recently used first), launches ready requests
 //              on free stream slots;
-//   builder -- creates the handles (planning + allocation) of admitted
+//   builders (kSrvBuilders) -- create the handles (planning + allocation) of admitted
 //              requests that need a new system, off the launch path, so the
 //              GPU keeps working while new systems are set up.
 // A request's life: queued -> building (new system) -> ready -> running -> done.
@@ -1360,7 +1360,8 @@ struct glst_server {
   std::unordered_map<uint64_t, bool> building_key;      // keys with a system under construction
   std::deque<SrvSlot> slots;  // stable addresses (stream callbacks point into it)
   std::vector<double *> old_pinned;    // outgrown staging, freed at destroy
-  std::thread worker, builder;
+  std::thread worker;
+  std::vector<std::thread> builders;  // kSrvBuilders, so small builds need not wait behind large ones
   bool stop = false;          // worker: finish what is queued, then exit
   bool stop_builder = false;  // builder: exit (set after the worker has finished)
   uint64_t next_ticket = 1, clock = 0;
@@ -1443,6 +1444,8 @@ static bool srv_admit(glst_server *s, SrvRequest *r) {
   s->cv_build.notify_one();
   return true;
 }
+
+static constexpr int kSrvBuilders = 2;
 
 static void srv_builder(glst_server *s) {
   cudaSetDevice(s->device);
@@ -1648,7 +1651,7 @@ glst_status glst_server_create(glst_server **out, uint64_t budget_bytes, uint32_
   }
   glst_server *raw = s.release();
   raw->worker = std::thread(srv_worker, raw);
-  raw->builder = std::thread(srv_builder, raw);
+  for (int i = 0; i < kSrvBuilders; i++) raw->builders.emplace_back(srv_builder, raw);
   *out = raw;
   return GLST_OK;
 }
@@ -1666,7 +1669,8 @@ glst_status glst_server_destroy(glst_server *s) {
     s->stop_builder = true;
   }
   s->cv_build.notify_all();
-  if (s->builder.joinable()) s->builder.join();
+  for (auto &b : s->builders)
+    if (b.joinable()) b.join();
   cudaSetDevice(s->device);
   cudaDeviceSynchronize();
   std::vector<SrvSystem *> left;
