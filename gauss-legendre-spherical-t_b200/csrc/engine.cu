@@ -495,8 +495,10 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
     h->sat_budget = budget;
     h->sat_nb = pow2_floor((uint32_t)std::max<size_t>(1, std::min<size_t>(8, budget / per_node)));
     // one process-wide maximum, so handles with different plans coexist
-    CUDA_TRY(cudaFuncSetAttribute(dev::k_shell_sums, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem_total));
+    CUDA_TRY(cudaFuncSetAttribute(dev::k_shell_sums<dev::kSatThreads, 3>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_total));
+    CUDA_TRY(cudaFuncSetAttribute(dev::k_shell_sums<dev::kSatThreadsOne, 1>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_total));
     h->nsm = nsm;
     h->g_node_base = node_base;
     h->g_dir_base = dir_base;
@@ -508,8 +510,9 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
       if (t.lr_waves) h->lr_waves = t.lr_waves;
     }
     GLST_TRY(build_chunks(h));
-    GLST_TRY(dalloc_n(h, &h->S, C * (size_t)h->K));
-    GLST_TRY(dalloc_n(h, &h->R, C * (size_t)h->K));
+    const size_t kpad = ((size_t)h->K + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock;
+    GLST_TRY(dalloc_n(h, &h->S, C * kpad));
+    GLST_TRY(dalloc_n(h, &h->R, C * kpad));
   }
   GLST_TRY(commit_allocs(h));
   if (K) {
@@ -568,7 +571,7 @@ static glst_status sf_range(glst_handle *h, uint32_t u0, uint32_t u1, cudaStream
   dim3 grid(u1 - u0, cg);
   dev::k_structure_factors<<<grid, dev::kSfThreads, 0, st>>>(h->pk, h->cell_count, h->cell_point, h->grid,
                                                               h->sf_units + u0, h->dirs, h->kappa,
-                                                              h->node64 + h->k_begin, h->K, h->S);
+                                                              h->node64 + h->k_begin, h->S);
   CUDA_TRY(cudaGetLastError());
   return GLST_OK;
 }
@@ -577,11 +580,16 @@ static glst_status shell_range(glst_handle *h, uint32_t kb, uint32_t ke, cudaStr
   if (ke <= kb || !h->plan.natom) return GLST_OK;
   uint32_t lg = 0;
   while ((1u << lg) < h->sat_nb) lg++;
-  dev::SatArgs a{h->S + kb, h->node64 + h->k_begin + kb, h->node_radii + h->k_begin + kb, ke - kb, h->K,
-                 h->sat_nb, lg, h->sat_xyz ? 1u : 0u, h->sat_stride, h->R + kb};
+  dev::SatArgs a{h->S, h->node64 + h->k_begin + kb, h->node_radii + h->k_begin + kb, ke - kb, kb,
+                 h->sat_nb, lg, h->sat_xyz ? 1u : 0u, h->sat_stride, h->R};
   const uint32_t nblk = (ke - kb + h->sat_nb - 1) / h->sat_nb;
   const size_t smem = h->sat_per_node * h->sat_nb + (h->sat_xyz ? (((size_t)h->plan.ncell * 4 + 15) & ~size_t(15)) : 0);
-  dev::k_shell_sums<<<nblk, dev::kSatThreads, smem, st>>>(h->grid, a);
+  // several nodes per CTA: 512 threads, 3 CTAs per SM; one node per CTA
+  // (large grids, one CTA fills the shared memory): 1024 threads
+  if (h->sat_nb == 1)
+    dev::k_shell_sums<dev::kSatThreadsOne, 1><<<nblk, dev::kSatThreadsOne, smem, st>>>(h->grid, a);
+  else
+    dev::k_shell_sums<dev::kSatThreads, 3><<<nblk, dev::kSatThreads, smem, st>>>(h->grid, a);
   CUDA_TRY(cudaGetLastError());
   return GLST_OK;
 }
@@ -590,7 +598,7 @@ static glst_status lr_range(glst_handle *h, uint32_t c0, uint32_t c1, cudaStream
   if (c1 <= c0 || !h->plan.natom) return GLST_OK;
   dim3 grid((h->plan.natom + dev::kLrThreads - 1) / dev::kLrThreads, c1 - c0);
   dev::k_long_range_flat<<<grid, dev::kLrThreads, 0, st>>>(
-      h->pk, h->cell_point, h->plan.ncell, h->chunks + c0, h->dirs, h->kappa, h->R, h->K, h->plan.natom,
+      h->pk, h->cell_point, h->plan.ncell, h->chunks + c0, h->dirs, h->kappa, h->R, h->plan.natom,
       h->part + (size_t)c0 * h->plan.natom);
   CUDA_TRY(cudaGetLastError());
   return GLST_OK;
@@ -1341,7 +1349,8 @@ uint64_t estimate_bytes(const Plan &p, int nsm) {
   if (K) {
     const uint64_t slots = (uint64_t)nsm * 16;
     const uint64_t chunks = std::max<uint64_t>(1, (8 * slots + C - 1) / C) + p.groups.size() + 1;
-    b += K * (32 + 4 + 16 + 4) + C * K * (16 + 8) + chunks * N * 32;
+    b += K * (32 + 4 + 16 + 4) + C * ((K + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock) * (16 + 8) +
+         chunks * N * 32;
   }
   return b + 64 * 16 * 64;  // per-buffer allocation granularity
 }

@@ -26,6 +26,18 @@ struct Grid {
   int ct_float;   // bin in float arithmetic (glst_force<float>)
 };
 
+// Layout of the structure factors S and shell sums R (C cells x K nodes):
+// blocks of kNodeBlock consecutive nodes, each block cell-major, so that a
+// cell's run of nodes is contiguous within a block (the structure-factor
+// stores and the long-range loads) and one node's values over all cells lie
+// in one C x kNodeBlock region (the shell-sum loads and stores; a plain
+// cell-major layout put them a whole row apart, one page per cell).
+// Buffers hold C x ceil(K / kNodeBlock) x kNodeBlock elements.
+constexpr uint32_t kNodeBlock = 32;
+__host__ __device__ __forceinline__ size_t sr_index(uint32_t c, uint32_t k, uint32_t ncell) {
+  return ((size_t)(k / kNodeBlock) * ncell + c) * kNodeBlock + (k % kNodeBlock);
+}
+
 // SFU sine and cosine of an FP32 angle in radians (PTX sin/cos.approx,
 // flush-to-zero).  Absolute error ~1e-6 for the |x| < ~30 rad used here,
 // below the FP32 rounding of the phase itself at that magnitude.
@@ -287,7 +299,7 @@ __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restric
                                         const uint32_t *__restrict__ cell_count,
                                         const uint32_t *__restrict__ cell_point, const Grid &g,
                                         const float4 *__restrict__ dirs, const float *__restrict__ kappa,
-                                        const double4 *__restrict__ node64, uint32_t ld, uint32_t c0,
+                                        const double4 *__restrict__ node64, uint32_t c0,
                                         uint32_t c1, double2 *__restrict__ S, float4 *s_at, float2 *s_f) {
   // Slots are handled in pairs (FMUL2/FFMA2); an odd last slot alone.
   constexpr int NP2 = NPT / 2;
@@ -376,7 +388,7 @@ __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restric
         const double sr = f.x, si = f.y;
         // (sr + i si) * (tc - i ts)
         const double2 v = make_double2(sr * tc + si * ts, si * tc - sr * ts);
-        double2 *dst = S + (size_t)cell * ld + k;
+        double2 *dst = S + sr_index(cell, k, g.ncell);
         if (a0 == 0) {
           *dst = v;
         } else {
@@ -395,14 +407,14 @@ __global__ void __launch_bounds__(kSfThreads, 6)
 k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_count,
                     const uint32_t *__restrict__ cell_point, Grid g, const SfUnit *__restrict__ units,
                     const float4 *__restrict__ dirs, const float *__restrict__ kappa,
-                    const double4 *__restrict__ node64, uint32_t ld, double2 *__restrict__ S) {
+                    const double4 *__restrict__ node64, double2 *__restrict__ S) {
   __shared__ float4 s_at[kSfAtomTile];
   __shared__ float2 s_f[kSfThreads * kSfMaxNpt];
   const SfUnit u = units[blockIdx.x];
   const uint32_t c0 = blockIdx.y * kSfCellsPerCta;
   const uint32_t c1 = min(g.ncell, c0 + kSfCellsPerCta);
 #define GLST_SF_CASE(n) \
-  case n: sf_unit<n>(u, pk, cell_count, cell_point, g, dirs, kappa, node64, ld, c0, c1, S, s_at, s_f); break;
+  case n: sf_unit<n>(u, pk, cell_count, cell_point, g, dirs, kappa, node64, c0, c1, S, s_at, s_f); break;
   switch (u.npt) {
     GLST_SF_CASE(1) GLST_SF_CASE(2) GLST_SF_CASE(3) GLST_SF_CASE(4) GLST_SF_CASE(5) GLST_SF_CASE(6)
     GLST_SF_CASE(7) GLST_SF_CASE(8) GLST_SF_CASE(9) GLST_SF_CASE(10) GLST_SF_CASE(11) GLST_SF_CASE(12)
@@ -419,13 +431,15 @@ k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ 
 // built from per-axis tables e^{i kx cx} e^{i ky cy} e^{i kz cz}.
 // CTA: nb nodes at once (rows of ncell+1 complex doubles in shared memory).
 constexpr int kSatThreads = 512;
+constexpr int kSatThreadsOne = 1024;  // one node per CTA (large grids): more warps per SM
+constexpr int kSatLoadBatch = 2;
 
 struct SatArgs {
   const double2 *S;
   const double4 *node64;        // (kx, ky, kz, w) FP64
   const uint32_t *node_radii;   // r_in | r_out << 16
   uint32_t K;                   // nodes handled by this launch
-  uint32_t ld;                  // row stride of S and R (nodes per cell row)
+  uint32_t kbase;               // local index of the launch's first node in S and R
   uint32_t nb;                  // nodes per CTA (a power of two, <= 32)
   uint32_t lg_nb;               // log2(nb)
   uint32_t xyz_table;           // 1: cell coordinates tabulated in shared memory
@@ -467,7 +481,8 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 // lines the warp takes per step, so the per-node values (radii, weight,
 // twiddle rows) stay in registers and the S loads and R stores of a warp are
 // runs of consecutive nodes.
-__global__ void __launch_bounds__(kSatThreads)
+template <int kThreads, int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
 k_shell_sums(Grid g, SatArgs a) {
   extern __shared__ double2 s_sat[];
   const uint32_t nb = a.nb, lg = a.lg_nb;
@@ -481,7 +496,8 @@ k_shell_sums(Grid g, SatArgs a) {
   const uint32_t per_warp = 32u >> lg;
   const uint32_t first = warp * per_warp + (lane >> lg);
   const uint32_t step = (blockDim.x >> 5) * per_warp;
-  const uint32_t k = k0 + j;
+  const uint32_t k = k0 + j;         // node within the launch (node tables)
+  const uint32_t ks = a.kbase + k;   // node within S and R
   const bool jv = k < a.K;
   // twiddle tables: e^{i k_a (i + 1/2) l} per node and axis
   for (uint32_t t = threadIdx.x; t < nb * naxis; t += blockDim.x) {
@@ -503,9 +519,20 @@ k_shell_sums(Grid g, SatArgs a) {
   if (a.xyz_table)
     for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) s_xyz[c] = coords(c);
   double2 *row = s_sat + (size_t)j * a.stride;
-  // S[c][k0 + j] -> row j
-  for (uint32_t c = first; c < C; c += step)
-    row[c] = jv ? a.S[(size_t)c * a.ld + k] : make_double2(0.0, 0.0);
+  // S[c][k0 + j] -> row j, kSatLoadBatch loads in flight per thread (one at a
+  // time left every thread waiting out a DRAM round trip per cell)
+  {
+    const double2 zero = make_double2(0.0, 0.0);
+    uint32_t c = first;
+    for (; c + (kSatLoadBatch - 1) * step < C; c += kSatLoadBatch * step) {
+      double2 v[kSatLoadBatch];
+#pragma unroll
+      for (int u = 0; u < kSatLoadBatch; u++) v[u] = jv ? __ldg(a.S + sr_index(c + u * step, ks, C)) : zero;
+#pragma unroll
+      for (int u = 0; u < kSatLoadBatch; u++) row[c + u * step] = v[u];
+    }
+    for (; c < C; c += step) row[c] = jv ? __ldg(a.S + sr_index(c, ks, C)) : zero;
+  }
   __syncthreads();
   // prefix along z (lines x, y)
   for (uint32_t l = first; l < g.nx * g.ny; l += step) {
@@ -545,7 +572,7 @@ k_shell_sums(Grid g, SatArgs a) {
     const double2 i = cube_sum(row, x, y, z, r_in, g);
     const double2 sh = make_double2((o.x - i.x) * w, (o.y - i.y) * w);
     const double2 r = cmul(cmul(sh, twx[x]), cmul(twy[y], twz[z]));
-    a.R[(size_t)c * a.ld + k] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
+    a.R[sr_index(c, ks, C)] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
   }
 }
 
@@ -611,7 +638,7 @@ __device__ __forceinline__ uint32_t cell_of_atom(const uint32_t *__restrict__ ce
 __global__ void __launch_bounds__(kLrThreads, 6)
 k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_point, uint32_t ncell,
                   const LrChunk *__restrict__ chunks, const float4 *__restrict__ dirs,
-                  const float *__restrict__ kappa, const float2 *__restrict__ R, uint32_t K, uint32_t natom,
+                  const float *__restrict__ kappa, const float2 *__restrict__ R, uint32_t natom,
                   double4 *__restrict__ part) {
   __shared__ float4 s_n[2][kLrfCells * kLrfSlot];
   __shared__ float2 s_kappa2[kLrfTilePairs];
@@ -652,9 +679,9 @@ k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ ce
         const uint32_t dd = i / npr, r = 2 * (i - dd * npr);
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (c < nc && dd < nd) {
-          const float2 *src = R + (size_t)(w0 + c) * K + ch.node_begin + (size_t)(d0 + dd) * nr + r;
-          const float2 x0 = src[0];
-          const float2 x1 = (r + 1 < nr) ? src[1] : make_float2(0.f, 0.f);
+          const uint32_t node = ch.node_begin + (d0 + dd) * nr + r;
+          const float2 x0 = R[sr_index(w0 + c, node, ncell)];
+          const float2 x1 = (r + 1 < nr) ? R[sr_index(w0 + c, node + 1, ncell)] : make_float2(0.f, 0.f);
           v = make_float4(x0.x, x1.x, x0.y, x1.y);
         }
         pre[k] = v;
