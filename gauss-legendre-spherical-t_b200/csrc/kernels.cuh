@@ -288,11 +288,12 @@ struct SfUnit {
 };
 
 // Slot pairs on the FMA pipe.  Per slot a polynomial costs ~21 FP32
-// operations and a MUFU slot 4 FP32 operations plus 2 MUFU operations, each of
-// which occupies the SFU for 8 cycles of a warp; the FMA and SFU pipes balance
-// at ~4 polynomial slots of 11.  Measured on water10k: 1.47 ms with none,
-// 1.28 ms with (npt - 1) / 4 pairs, 1.39 ms with (npt + 1) / 4.
-__host__ __device__ constexpr int sf_poly_pairs(int npt) { return (npt - 1) / 4; }
+// operations and a SFU slot 4 FP32 operations plus 2 MUFU operations, each of
+// which occupies the SFU for 8 cycles of a warp.  Measured on water10k
+// (npt 11 / 9 / 10 in its three groups): SF 1.47 ms with no pairs, 1.31 ms
+// with (npt - 1) / 4 (2/2/2), 1.25 ms with (npt - 3) / 4 (2/1/1), 1.28 ms
+// with one pair everywhere, 1.29 ms with (npt - 3) / 3 (2/2/2 + ...).
+__host__ __device__ constexpr int sf_poly_pairs(int npt) { return (npt - 3) / 4; }
 
 template <int NPT>
 __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restrict__ pk,
