@@ -236,7 +236,9 @@ def run_serve(g, n_requests=120, loads=(0.5, 0.8, 1.1), budget=150 << 30, nslots
     N(0, 0.01 A); HBM budget 150 GB.  Capacity = requests/s with every
     request queued at once; then Poisson arrivals at 3 offered loads (fractions
     of that capacity), continuous batching (8 slots) vs one request at a time
-    (1 slot).  Latency = submit to completion."""
+    (1 slot).  Latency = submit to completion.  Each figure is the median
+    (by throughput) of three runs; every run starts a new server, so its new
+    systems are planned and allocated inside the run."""
     from glst_b200 import systems
     reqs = systems.request_stream(n_requests, seed=seed)
     atoms = sum(len(r["x"]) for r in reqs)
@@ -258,10 +260,17 @@ def run_serve(g, n_requests=120, loads=(0.5, 0.8, 1.1), budget=150 << 30, nslots
                 "value": atoms / span, "requests_per_s": len(lat) / span,
                 "evictions": int(st.evictions), "systems_created": int(st.systems_created)}
 
+    def median_of(runs, nslots_, arrivals):
+        # shared-box timing of ~1 s runs is noisy: the run with the median span
+        res = sorted((serve(nslots_, arrivals) for _ in range(runs)), key=lambda r: r["requests_per_s"])
+        out = dict(res[len(res) // 2])
+        out["runs"] = runs
+        return out
+
     zero = [0.0] * len(reqs)
     serve(nslots, zero)  # warm-up pass: plans, pinned staging, first kernel launches
-    cap = serve(nslots, zero)
-    cap_plain = serve(1, zero)
+    cap = median_of(3, nslots, zero)
+    cap_plain = median_of(3, 1, zero)
     rng = np.random.default_rng(seed + 1)
     out = {"workload": "%d requests, %d atoms, 1,000-200,000 atoms each, 60%% continue a resident system"
                        % (len(reqs), atoms), "unit": UNIT, "budget_bytes": budget,
@@ -269,8 +278,8 @@ def run_serve(g, n_requests=120, loads=(0.5, 0.8, 1.1), budget=150 << 30, nslots
     for f in loads:
         rate = f * cap["requests_per_s"]
         arr = np.cumsum(rng.exponential(1.0 / rate, len(reqs))).tolist()
-        out["loads"].append({"offered": f, "rate_per_s": rate, "continuous_batching": serve(nslots, arr),
-                             "one_at_a_time": serve(1, arr)})
+        out["loads"].append({"offered": f, "rate_per_s": rate, "continuous_batching": median_of(3, nslots, arr),
+                             "one_at_a_time": median_of(3, 1, arr)})
     return out
 
 
