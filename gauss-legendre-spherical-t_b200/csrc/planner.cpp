@@ -80,6 +80,7 @@ std::shared_ptr<TDesignStore> TDesignStore::open(const std::string &path) {
 }
 
 const std::vector<double> *TDesignStore::get(unsigned t) {
+  std::lock_guard<std::mutex> lk(mu_);
   auto it = cache_.find(t);
   if (it != cache_.end()) return &it->second;
   if (!is_dir_) return nullptr;

@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <string>
 #include <vector>
@@ -32,7 +33,8 @@ class TDesignStore {
   bool is_dir_ = false;
   std::map<unsigned, std::string> files_;  // degree -> file (dir layout)
   std::map<unsigned, unsigned> file_m_;    // degree -> N/2 (dir layout)
-  std::map<unsigned, std::vector<double>> cache_;
+  std::map<unsigned, std::vector<double>> cache_;  // node-based: pointers stay valid
+  std::mutex mu_;  // get() fills cache_ lazily (directory layout) from any thread
 };
 
 struct GroupPlan {
