@@ -1386,14 +1386,26 @@ struct glst_server {
   bool stop_builder = false;  // builder: exit (set after the worker has finished)
   uint64_t next_ticket = 1, clock = 0;
   uint64_t reserved = 0;               // bytes promised to systems being built
+  std::deque<SrvSystem *> to_free;     // dropped systems, freed by a builder thread
+  uint64_t freeing = 0;                // their bytes, until freed
   uint32_t large_in_flight = 0;        // running requests of >= kSrvSmallAtoms atoms
   glst_server_stats stats{};
 };
 
+// Take a system out of service (lock held).  Its device memory is freed by
+// a builder thread, outside the lock: cudaFree waits for the whole device,
+// which in the worker would stall every launch behind it.  Until then its
+// bytes count against the budget as `freeing`.
 static void srv_drop_system(glst_server *s, SrvSystem *sys) {
   if (sys->key) s->resident.erase(sys->key);
   s->stats.resident_bytes -= sys->bytes;
   s->stats.resident_systems--;
+  s->freeing += sys->bytes;
+  s->to_free.push_back(sys);
+  s->cv_build.notify_one();
+}
+
+static void srv_free_now(SrvSystem *sys) {
   release(sys->h);
   delete sys->h;
   delete sys;
@@ -1410,11 +1422,11 @@ static void srv_finish(glst_server *s, SrvRequest *r, glst_status st, const char
 
 // Evict idle named systems, least recently used first, until `need` fits.
 static bool srv_make_room(glst_server *s, uint64_t need) {
-  while (s->stats.resident_bytes + s->reserved + need > s->budget) {
+  while (s->stats.resident_bytes + s->reserved + s->freeing + need > s->budget) {
     SrvSystem *victim = nullptr;
     for (auto &kv : s->resident)
       if (!kv.second->busy && (!victim || kv.second->last_use < victim->last_use)) victim = kv.second;
-    if (!victim) return false;
+    if (!victim) return false;  // running requests (or pending frees) will make room
     srv_drop_system(s, victim);
     s->stats.evictions++;
   }
@@ -1471,7 +1483,18 @@ static void srv_builder(glst_server *s) {
   cudaSetDevice(s->device);
   std::unique_lock<std::mutex> lk(s->mu);
   while (true) {
-    s->cv_build.wait(lk, [&] { return s->stop_builder || !s->to_build.empty(); });
+    s->cv_build.wait(lk, [&] { return s->stop_builder || !s->to_build.empty() || !s->to_free.empty(); });
+    if (!s->to_free.empty()) {  // frees first: builds may be waiting for the memory
+      SrvSystem *sys = s->to_free.front();
+      s->to_free.pop_front();
+      const uint64_t b = sys->bytes;
+      lk.unlock();
+      srv_free_now(sys);
+      lk.lock();
+      s->freeing -= b;
+      s->cv_work.notify_all();
+      continue;
+    }
     if (s->to_build.empty()) {
       if (s->stop_builder) break;
       continue;
@@ -1693,9 +1716,9 @@ glst_status glst_server_destroy(glst_server *s) {
     if (b.joinable()) b.join();
   cudaSetDevice(s->device);
   cudaDeviceSynchronize();
-  std::vector<SrvSystem *> left;
+  std::vector<SrvSystem *> left(s->to_free.begin(), s->to_free.end());
   for (auto &kv : s->resident) left.push_back(kv.second);
-  for (auto *sys : left) srv_drop_system(s, sys);
+  for (auto *sys : left) srv_free_now(sys);
   for (auto &sl : s->slots) {
     if (sl.pin) cudaFreeHost(sl.pin);
     cudaStreamDestroy(sl.st);
