@@ -246,13 +246,14 @@ static Tuning tuned(const Plan &p, uint32_t K) {
   return it == g_tune.end() ? Tuning{} : it->second;
 }
 
+static constexpr uint32_t kFarStages = 1;  // far-field pipeline stages per solve (see below)
+
 static uint32_t pow2_floor(uint32_t v) {
   uint32_t p = 1;
   while (p * 2 <= v && p < 32) p *= 2;
   return p;
 }
 
-static constexpr uint32_t kFarStages = 1;  // far-field pipeline stages per solve (see below)
 
 // Long-range chunks: whole directions of one group each, sized so that
 // ncell x chunks is about lr_waves waves of resident CTAs; then this
@@ -385,6 +386,30 @@ static glst_status build_chunks(glst_handle *h) {
   return GLST_OK;
 }
 
+// Kernel attributes (the opt-in shared-memory maxima) are set once per
+// device and process, with one process-wide value, so handles with different
+// plans coexist.  Setting them for every new handle cost servers time: the
+// call can wait while the same kernels run on other streams.
+static glst_status set_kernel_attributes(int device, size_t shell_smem) {
+  static std::mutex mu;
+  static std::map<int, int> done;  // device -> bit 1: sort, bit 2: shell sums
+  std::lock_guard<std::mutex> lk(mu);
+  int &d = done[device];
+  if (!(d & 1)) {
+    CUDA_TRY(cudaFuncSetAttribute(dev::k_sort_pack, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(dev::kSortCap * sizeof(uint32_t))));
+    d |= 1;
+  }
+  if (shell_smem && !(d & 2)) {
+    CUDA_TRY(cudaFuncSetAttribute(dev::k_shell_sums<dev::kSatThreads, 3>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shell_smem));
+    CUDA_TRY(cudaFuncSetAttribute(dev::k_shell_sums<dev::kSatThreadsOne, 1>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shell_smem));
+    d |= 2;
+  }
+  return GLST_OK;
+}
+
 static glst_status setup(glst_handle *h, uint32_t natom, double tol,
                          const double box[3], double rcut, int ct_float,
                          uint32_t shard = 0, uint32_t nshards = 1) {
@@ -494,11 +519,7 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
     h->sat_per_node = per_node;
     h->sat_budget = budget;
     h->sat_nb = pow2_floor((uint32_t)std::max<size_t>(1, std::min<size_t>(8, budget / per_node)));
-    // one process-wide maximum, so handles with different plans coexist
-    CUDA_TRY(cudaFuncSetAttribute(dev::k_shell_sums<dev::kSatThreads, 3>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_total));
-    CUDA_TRY(cudaFuncSetAttribute(dev::k_shell_sums<dev::kSatThreadsOne, 1>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_total));
+    GLST_TRY(set_kernel_attributes(h->device, smem_total));
     h->nsm = nsm;
     h->g_node_base = node_base;
     h->g_dir_base = dir_base;
@@ -522,8 +543,7 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
     CUDA_TRY(cudaMemcpy(h->kappa, kap.data(), kap.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
   if (shard > 0) CUDA_TRY(cudaMemset(h->sr, 0, (size_t)dev::kSrPlanes * N * sizeof(double4)));
-  CUDA_TRY(cudaFuncSetAttribute(dev::k_sort_pack, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(dev::kSortCap * sizeof(uint32_t))));
+  GLST_TRY(set_kernel_attributes(h->device, 0));
   CUDA_TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
   CUDA_TRY(cudaStreamCreateWithFlags(&h->far2, cudaStreamNonBlocking));
   CUDA_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
@@ -1479,6 +1499,11 @@ static bool srv_admit(glst_server *s, SrvRequest *r) {
 
 static constexpr int kSrvBuilders = 2;
 
+// Requests of at least this many atoms fill the GPU by themselves.  (Running
+// their far field in 8 node ranges, so that smaller requests could start
+// between the ranges' launches, measured no better p50 and a worse p99.)
+static constexpr uint32_t kSrvSmallAtoms = 20000;
+
 static void srv_builder(glst_server *s) {
   cudaSetDevice(s->device);
   std::unique_lock<std::mutex> lk(s->mu);
@@ -1551,8 +1576,6 @@ static void CUDART_CB srv_done_cb(void *arg) {
   sl->owner->cv_work.notify_all();
 }
 
-// Requests of at least this many atoms fill the GPU by themselves.
-static constexpr uint32_t kSrvSmallAtoms = 20000;
 
 // Launch a ready request on a free slot (lock held).  All slots have equal
 // stream priority: giving small requests priority starved the large ones
