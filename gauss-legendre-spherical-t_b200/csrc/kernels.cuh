@@ -636,7 +636,7 @@ __device__ __forceinline__ uint32_t cell_of_atom(const uint32_t *__restrict__ ce
   return lo;
 }
 
-__global__ void __launch_bounds__(kLrThreads, 6)
+__global__ void __launch_bounds__(kLrThreads, 8)
 k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_point, uint32_t ncell,
                   const LrChunk *__restrict__ chunks, const float4 *__restrict__ dirs,
                   const float *__restrict__ kappa, const float2 *__restrict__ R, uint32_t natom,
