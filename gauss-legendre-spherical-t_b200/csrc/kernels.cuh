@@ -404,7 +404,7 @@ __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restric
 
 // node64 and S are offset to the launch's first local node; units index
 // them from there.
-__global__ void __launch_bounds__(kSfThreads, 6)
+__global__ void __launch_bounds__(kSfThreads, 8)
 k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_count,
                     const uint32_t *__restrict__ cell_point, Grid g, const SfUnit *__restrict__ units,
                     const float4 *__restrict__ dirs, const float *__restrict__ kappa,
