@@ -115,7 +115,6 @@ struct glst_handle {
   uint32_t k_begin = 0;             // first node (internal order) of this shard
   uint32_t lr_waves = 8;            // long-range CTAs ~ lr_waves x resident slots
   size_t part_cap = 0;              // rows the part buffer holds
-  size_t chunk_bytes = 0;
   size_t sat_per_node = 0;          // shell-sum shared bytes per node
   size_t sat_budget = 0;            // shell-sum shared bytes per CTA, at most
   int nsm = 148;
@@ -144,7 +143,10 @@ struct glst_handle {
   float *kappa = nullptr;       // radial scales per group, FP32
   dev::LrChunk *chunks = nullptr;
   dev::SfUnit *sf_units = nullptr;  // structure-factor work units (whole directions)
-  size_t sf_unit_bytes = 0;
+  size_t chunk_cap = 0, unit_cap = 0;         // entries the tables hold
+  bool chunks_owned = false, units_owned = false, part_owned = false;  // own cudaMalloc (else arena)
+  std::vector<dev::LrChunk> host_chunks;      // set-up: uploaded after the arena is committed
+  std::vector<dev::SfUnit> host_units;
   uint32_t n_sf_units = 0;
   // far field
   double2 *S = nullptr;
@@ -208,13 +210,14 @@ static void release(glst_handle *h) {
   for (auto &b : h->bufs) cudaFree(b.p);
   h->bufs.clear();
   h->pending.clear();
-  if (h->chunks) cudaFree(h->chunks);
-  if (h->sf_units) cudaFree(h->sf_units);
-  if (h->part) cudaFree(h->part);
+  if (h->chunks_owned && h->chunks) cudaFree(h->chunks);
+  if (h->units_owned && h->sf_units) cudaFree(h->sf_units);
+  if (h->part_owned && h->part) cudaFree(h->part);
   h->chunks = nullptr;
   h->sf_units = nullptr;
   h->part = nullptr;
-  h->part_cap = 0;
+  h->chunks_owned = h->units_owned = h->part_owned = false;
+  h->chunk_cap = h->unit_cap = h->part_cap = 0;
   h->bytes = 0;
   if (h->side) cudaStreamDestroy(h->side);
   if (h->far2) cudaStreamDestroy(h->far2);
@@ -258,7 +261,7 @@ static uint32_t pow2_floor(uint32_t v) {
 // Long-range chunks: whole directions of one group each, sized so that
 // ncell x chunks is about lr_waves waves of resident CTAs; then this
 // device's share when the system is split over several devices.
-static glst_status build_chunks(glst_handle *h) {
+static glst_status build_chunks(glst_handle *h, bool in_arena = false) {
   const Plan &p = h->plan;
   const size_t C = p.ncell, K = p.has_far ? p.K() : 0, N = p.natom;
   const size_t slots = (size_t)h->nsm * 16;
@@ -349,40 +352,50 @@ static glst_status build_chunks(glst_handle *h) {
   }
   h->n_sf_units = (uint32_t)units.size();
   if (units.size() > 0x7FFFFFFFu) return fail(GLST_ERR_SIZE, "too many structure-factor units");
-  if (h->chunks) {
-    cudaFree(h->chunks);
-    h->bytes -= h->chunk_bytes;
+  const size_t part_rows = std::max<size_t>(1, h->nsplit);
+  if (in_arena) {
+    // first build (set-up): carve the tables and partial rows out of the
+    // handle's single allocation; uploaded once it is committed.  Separate
+    // small cudaMalloc calls here took 25-270 ms while a server's other
+    // requests kept the GPU busy.
+    GLST_TRY(dalloc_n(h, &h->chunks, std::max<size_t>(1, chunks.size())));
+    GLST_TRY(dalloc_n(h, &h->sf_units, std::max<size_t>(1, units.size())));
+    GLST_TRY(dalloc_n(h, &h->part, part_rows * std::max<size_t>(1, N)));
+    h->chunk_cap = std::max<size_t>(1, chunks.size());
+    h->unit_cap = std::max<size_t>(1, units.size());
+    h->part_cap = part_rows;
+    h->host_chunks = std::move(chunks);
+    h->host_units = std::move(units);
+    return GLST_OK;
   }
-  h->chunks = nullptr;
-  h->sf_units = nullptr;
-  h->chunk_bytes = 0;
-  if (h->sf_units) {
-    cudaFree(h->sf_units);
-    h->bytes -= h->sf_unit_bytes;
-  }
-  h->sf_units = nullptr;
-  h->sf_unit_bytes = 0;
-  if (!chunks.empty()) {
-    h->chunk_bytes = chunks.size() * sizeof(dev::LrChunk);
-    CUDA_TRY(cudaMalloc(&h->chunks, h->chunk_bytes));
-    h->bytes += h->chunk_bytes;
-    CUDA_TRY(cudaMemcpy(h->chunks, chunks.data(), h->chunk_bytes, cudaMemcpyHostToDevice));
-    h->sf_unit_bytes = units.size() * sizeof(dev::SfUnit);
-    CUDA_TRY(cudaMalloc(&h->sf_units, h->sf_unit_bytes));
-    h->bytes += h->sf_unit_bytes;
-    CUDA_TRY(cudaMemcpy(h->sf_units, units.data(), h->sf_unit_bytes, cudaMemcpyHostToDevice));
-  }
-  if ((size_t)h->nsplit > h->part_cap) {
-    if (h->part) {
-      cudaFree(h->part);
-      h->bytes -= h->part_cap * N * sizeof(double4);
+  // rebuild (autotune): reuse the buffers when the new tables fit, else
+  // allocate larger ones of their own
+  auto regrow = [&](void **buf, bool &owned, size_t &cap, size_t need, size_t elem) -> glst_status {
+    if (need <= cap) return GLST_OK;
+    if (owned && *buf) {
+      cudaFree(*buf);
+      h->bytes -= cap * elem;
     }
-    h->part = nullptr;
-    h->part_cap = 0;
-    CUDA_TRY(cudaMalloc(&h->part, std::max<size_t>(1, (size_t)h->nsplit * N) * sizeof(double4)));
-    h->part_cap = h->nsplit;
-    h->bytes += h->part_cap * N * sizeof(double4);
-  }
+    *buf = nullptr;
+    cap = 0;
+    owned = true;
+    CUDA_TRY(cudaMalloc(buf, need * elem));
+    cap = need;
+    h->bytes += need * elem;
+    return GLST_OK;
+  };
+  GLST_TRY(regrow(reinterpret_cast<void **>(&h->chunks), h->chunks_owned, h->chunk_cap,
+                  std::max<size_t>(1, chunks.size()), sizeof(dev::LrChunk)));
+  GLST_TRY(regrow(reinterpret_cast<void **>(&h->sf_units), h->units_owned, h->unit_cap,
+                  std::max<size_t>(1, units.size()), sizeof(dev::SfUnit)));
+  size_t part_cap_elems = h->part_cap * std::max<size_t>(1, N);
+  GLST_TRY(regrow(reinterpret_cast<void **>(&h->part), h->part_owned, part_cap_elems,
+                  part_rows * std::max<size_t>(1, N), sizeof(double4)));
+  h->part_cap = part_cap_elems / std::max<size_t>(1, N);
+  if (!chunks.empty())
+    CUDA_TRY(cudaMemcpy(h->chunks, chunks.data(), chunks.size() * sizeof(dev::LrChunk), cudaMemcpyHostToDevice));
+  if (!units.empty())
+    CUDA_TRY(cudaMemcpy(h->sf_units, units.data(), units.size() * sizeof(dev::SfUnit), cudaMemcpyHostToDevice));
   return GLST_OK;
 }
 
@@ -530,12 +543,20 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
         h->sat_nb = pow2_floor(std::min<uint32_t>(t.sat_nb, (uint32_t)std::max<size_t>(1, budget / per_node)));
       if (t.lr_waves) h->lr_waves = t.lr_waves;
     }
-    GLST_TRY(build_chunks(h));
+    GLST_TRY(build_chunks(h, /*in_arena=*/true));
     const size_t kpad = ((size_t)h->K + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock;
     GLST_TRY(dalloc_n(h, &h->S, C * kpad));
     GLST_TRY(dalloc_n(h, &h->R, C * kpad));
   }
   GLST_TRY(commit_allocs(h));
+  if (!h->host_chunks.empty()) {
+    CUDA_TRY(cudaMemcpy(h->chunks, h->host_chunks.data(), h->host_chunks.size() * sizeof(dev::LrChunk),
+                        cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->sf_units, h->host_units.data(), h->host_units.size() * sizeof(dev::SfUnit),
+                        cudaMemcpyHostToDevice));
+  }
+  h->host_chunks.clear();
+  h->host_units.clear();
   if (K) {
     CUDA_TRY(cudaMemcpy(h->node64, n64.data(), K * sizeof(double4), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(h->node_radii, radii.data(), K * sizeof(uint32_t), cudaMemcpyHostToDevice));
