@@ -178,17 +178,48 @@ static glst_status dalloc(glst_handle *h, void **out, size_t bytes) {
   return GLST_OK;
 }
 
+// Handle memory comes from one stream-ordered pool per device that keeps
+// freed blocks for later handles (release threshold: unlimited).  Plain
+// cudaMalloc calls took ~25 ms each, and held up other threads' CUDA calls,
+// while a server's requests kept the GPU busy; a pool that already holds
+// the memory hands it out without touching the device's page tables.
+static glst_status handle_pool(int device, cudaMemPool_t *pool) {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = pools.find(device);
+  if (it != pools.end()) {
+    *pool = it->second;
+    return GLST_OK;
+  }
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  cudaMemPool_t p = nullptr;
+  CUDA_TRY(cudaMemPoolCreate(&p, &props));
+  uint64_t keep = ~0ull;
+  CUDA_TRY(cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep));
+  pools[device] = p;
+  *pool = p;
+  return GLST_OK;
+}
+
 static glst_status commit_allocs(glst_handle *h) {
   auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
   size_t total = 0;
   for (const auto &p : h->pending) total += al(p.bytes);
   if (!total) return GLST_OK;
   void *base = nullptr;
-  const cudaError_t e = cudaMalloc(&base, total);
+  cudaMemPool_t pool = nullptr;
+  GLST_TRY(handle_pool(h->device, &pool));
+  // ordered on the handle's side stream; set-up synchronises it before
+  // returning, after which any stream may use the memory
+  const cudaError_t e = cudaMallocFromPoolAsync(&base, total, pool, h->side);
   if (e != cudaSuccess) {
     cudaGetLastError();
     h->pending.clear();
-    return fail(GLST_ERR_OUT_OF_MEMORY, "cudaMalloc(%zu bytes) failed: %s", total, cudaGetErrorString(e));
+    return fail(GLST_ERR_OUT_OF_MEMORY, "device allocation of %zu bytes failed: %s", total, cudaGetErrorString(e));
   }
   h->bufs.push_back({base, total});
   h->bytes += total;
@@ -206,8 +237,12 @@ static glst_status dalloc_n(glst_handle *h, T **out, size_t n) {
   return dalloc(h, reinterpret_cast<void **>(out), n * sizeof(T));
 }
 
-static void release(glst_handle *h) {
-  for (auto &b : h->bufs) cudaFree(b.p);
+// `device_idle`: the caller knows no work on this handle's memory is in
+// flight (a server's idle system); otherwise the device is synchronised
+// first, as cudaFree would, before the memory goes back to the pool.
+static void release(glst_handle *h, bool device_idle = false) {
+  if (!h->bufs.empty() && !device_idle) cudaDeviceSynchronize();
+  for (auto &b : h->bufs) cudaFreeAsync(b.p, h->side);
   h->bufs.clear();
   h->pending.clear();
   if (h->chunks_owned && h->chunks) cudaFree(h->chunks);
@@ -435,6 +470,11 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
     return fail(GLST_ERR_NO_DEVICE, "no CUDA capable device found");
   }
   CUDA_TRY(cudaGetDevice(&h->device));
+  CUDA_TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+  CUDA_TRY(cudaStreamCreateWithFlags(&h->far2, cudaStreamNonBlocking));
+  CUDA_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&h->ev_far2, cudaEventDisableTiming));
   try {
     auto store = get_store();
     h->plan = glst::make_plan(natom, tol, box, rcut, ct_float, *store);
@@ -550,27 +590,23 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
   }
   GLST_TRY(commit_allocs(h));
   if (!h->host_chunks.empty()) {
-    CUDA_TRY(cudaMemcpy(h->chunks, h->host_chunks.data(), h->host_chunks.size() * sizeof(dev::LrChunk),
-                        cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(h->sf_units, h->host_units.data(), h->host_units.size() * sizeof(dev::SfUnit),
-                        cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpyAsync(h->chunks, h->host_chunks.data(), h->host_chunks.size() * sizeof(dev::LrChunk),
+                             cudaMemcpyHostToDevice, h->side));
+    CUDA_TRY(cudaMemcpyAsync(h->sf_units, h->host_units.data(), h->host_units.size() * sizeof(dev::SfUnit),
+                             cudaMemcpyHostToDevice, h->side));
   }
   h->host_chunks.clear();
   h->host_units.clear();
   if (K) {
-    CUDA_TRY(cudaMemcpy(h->node64, n64.data(), K * sizeof(double4), cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(h->node_radii, radii.data(), K * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(h->dirs, dirs.data(), dirs.size() * sizeof(float4), cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(h->kappa, kap.data(), kap.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpyAsync(h->node64, n64.data(), K * sizeof(double4), cudaMemcpyHostToDevice, h->side));
+    CUDA_TRY(cudaMemcpyAsync(h->node_radii, radii.data(), K * sizeof(uint32_t), cudaMemcpyHostToDevice, h->side));
+    CUDA_TRY(cudaMemcpyAsync(h->dirs, dirs.data(), dirs.size() * sizeof(float4), cudaMemcpyHostToDevice, h->side));
+    CUDA_TRY(cudaMemcpyAsync(h->kappa, kap.data(), kap.size() * sizeof(float), cudaMemcpyHostToDevice, h->side));
   }
-  if (shard > 0) CUDA_TRY(cudaMemset(h->sr, 0, (size_t)dev::kSrPlanes * N * sizeof(double4)));
+  if (shard > 0) CUDA_TRY(cudaMemsetAsync(h->sr, 0, (size_t)dev::kSrPlanes * N * sizeof(double4), h->side));
   GLST_TRY(set_kernel_attributes(h->device, 0));
-  CUDA_TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
-  CUDA_TRY(cudaStreamCreateWithFlags(&h->far2, cudaStreamNonBlocking));
-  CUDA_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
-  CUDA_TRY(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
-  CUDA_TRY(cudaEventCreateWithFlags(&h->ev_far2, cudaEventDisableTiming));
-  CUDA_TRY(cudaMemset(h->flags, 0, 4 * sizeof(uint32_t)));
+  CUDA_TRY(cudaMemsetAsync(h->flags, 0, 4 * sizeof(uint32_t), h->side));
+  CUDA_TRY(cudaStreamSynchronize(h->side));  // memory and tables ready for any stream
   h->computed = false;
   return GLST_OK;
 }
@@ -1447,7 +1483,7 @@ static void srv_drop_system(glst_server *s, SrvSystem *sys) {
 }
 
 static void srv_free_now(SrvSystem *sys) {
-  release(sys->h);
+  release(sys->h, /*device_idle=*/true);  // its last request has completed
   delete sys->h;
   delete sys;
 }
@@ -1551,7 +1587,7 @@ static void srv_builder(glst_server *s) {
     auto h = std::make_unique<glst_handle>();
     const glst_status st = setup(h.get(), r->natom, r->tol, r->box, r->rcut, 0);
     const std::string err = st == GLST_OK ? std::string() : g_last_error;
-    if (st != GLST_OK) release(h.get());
+    if (st != GLST_OK) release(h.get(), /*device_idle=*/true);  // nothing ran on it
     lk.lock();
     s->reserved -= r->reserved;
     r->reserved = 0;
