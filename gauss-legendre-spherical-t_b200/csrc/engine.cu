@@ -859,7 +859,7 @@ glst_status glst_destroy(glst_handle *h) {
   if (!h) return GLST_OK;
   DeviceGuard guard_(h);
   cudaDeviceSynchronize();
-  release(h);
+  release(h, /*device_idle=*/true);
   delete h;
   return GLST_OK;
 }
@@ -1179,9 +1179,10 @@ static void batch_release(glst_batch *b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   b->exec = nullptr;
   b->graph = nullptr;
+  if (!b->sys.empty()) cudaDeviceSynchronize();
   for (auto *h : b->sys) {
     if (h) {
-      release(h);
+      release(h, /*device_idle=*/true);
       delete h;
     }
   }
