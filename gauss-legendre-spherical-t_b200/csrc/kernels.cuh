@@ -433,7 +433,7 @@ k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ 
 // CTA: nb nodes at once (rows of ncell+1 complex doubles in shared memory).
 constexpr int kSatThreads = 512;
 constexpr int kSatThreadsOne = 1024;  // one node per CTA (large grids): more warps per SM
-constexpr int kSatLoadBatch = 2;
+constexpr int kSatLoadBatch = 4;
 
 struct SatArgs {
   const double2 *S;
@@ -520,26 +520,30 @@ k_shell_sums(Grid g, SatArgs a) {
   if (a.xyz_table)
     for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) s_xyz[c] = coords(c);
   double2 *row = s_sat + (size_t)j * a.stride;
-  // S[c][k0 + j] -> row j, kSatLoadBatch loads in flight per thread (one at a
-  // time left every thread waiting out a DRAM round trip per cell)
+  // S[c][k0 + j] -> row j, summed along z on the way in (the z prefix pass
+  // without its own shared-memory round trip); kSatLoadBatch loads of a line
+  // in flight per thread (one at a time left every thread waiting out a DRAM
+  // round trip per cell)
   {
     const double2 zero = make_double2(0.0, 0.0);
-    uint32_t c = first;
-    for (; c + (kSatLoadBatch - 1) * step < C; c += kSatLoadBatch * step) {
-      double2 v[kSatLoadBatch];
+    for (uint32_t l = first; l < g.nx * g.ny; l += step) {
+      const uint32_t base = l * g.nz;
+      double2 acc = zero;
+      for (uint32_t z0 = 0; z0 < g.nz; z0 += kSatLoadBatch) {
+        double2 v[kSatLoadBatch];
 #pragma unroll
-      for (int u = 0; u < kSatLoadBatch; u++) v[u] = jv ? __ldg(a.S + sr_index(c + u * step, ks, C)) : zero;
+        for (int u = 0; u < kSatLoadBatch; u++)
+          v[u] = (jv && z0 + u < g.nz) ? __ldg(a.S + sr_index(base + z0 + u, ks, C)) : zero;
 #pragma unroll
-      for (int u = 0; u < kSatLoadBatch; u++) row[c + u * step] = v[u];
+        for (int u = 0; u < kSatLoadBatch; u++) {
+          if (z0 + u < g.nz) {
+            acc.x += v[u].x;
+            acc.y += v[u].y;
+            row[base + z0 + u] = acc;
+          }
+        }
+      }
     }
-    for (; c < C; c += step) row[c] = jv ? __ldg(a.S + sr_index(c, ks, C)) : zero;
-  }
-  __syncthreads();
-  // prefix along z (lines x, y)
-  for (uint32_t l = first; l < g.nx * g.ny; l += step) {
-    double2 *p = row + l * g.nz;
-    double2 acc = make_double2(0.0, 0.0);
-    for (uint32_t z = 0; z < g.nz; z++) { acc.x += p[z].x; acc.y += p[z].y; p[z] = acc; }
   }
   __syncthreads();
   // prefix along y (lines x, z)
