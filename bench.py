@@ -425,11 +425,10 @@ def run_ours(args, world, rank, local, dist):
         "fp32_fma_peak_per_s": fma_peak,
     }
     # The same kernel against the HBM roofline (MEASURED_PEAKS.json): its
-    # algorithmic bytes are the cross-cell operand it streams once (R read,
-    # C x K float2, for the gather; S written, C x K double2, for the
-    # structure factors).
+    # algorithmic bytes are the cross-cell operand it streams once (R read
+    # for the gather, S written for the structure factors: C x K float2).
     C = inf.ncell_total
-    hbm_bytes = C * K * (8.0 if dom == "long_range" else 16.0)
+    hbm_bytes = C * K * 8.0
     hbm_peak, hbm_src = 6650.0, "fallback (no MEASURED_PEAKS.json)"
     mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(mp):

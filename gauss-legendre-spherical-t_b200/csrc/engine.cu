@@ -149,7 +149,7 @@ struct glst_handle {
   std::vector<dev::SfUnit> host_units;
   uint32_t n_sf_units = 0;
   // far field
-  double2 *S = nullptr;
+  float2 *S = nullptr;
   float2 *R = nullptr;
   double4 *part = nullptr;
   double4 *sr = nullptr;
@@ -647,8 +647,7 @@ static glst_status sf_range(glst_handle *h, uint32_t u0, uint32_t u1, cudaStream
   if (cg > 65535) return fail(GLST_ERR_SIZE, "too many cells for the structure-factor grid");
   dim3 grid(u1 - u0, cg);
   dev::k_structure_factors<<<grid, dev::kSfThreads, 0, st>>>(h->pk, h->cell_count, h->cell_point, h->grid,
-                                                              h->sf_units + u0, h->dirs, h->kappa,
-                                                              h->node64 + h->k_begin, h->S);
+                                                              h->sf_units + u0, h->dirs, h->kappa, h->S);
   CUDA_TRY(cudaGetLastError());
   return GLST_OK;
 }
@@ -1438,7 +1437,7 @@ uint64_t estimate_bytes(const Plan &p, int nsm) {
   if (K) {
     const uint64_t slots = (uint64_t)nsm * 16;
     const uint64_t chunks = std::max<uint64_t>(1, (8 * slots + C - 1) / C) + p.groups.size() + 1;
-    b += K * (32 + 4 + 16 + 4) + C * ((K + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock) * (16 + 8) +
+    b += K * (32 + 4 + 16 + 4) + C * ((K + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock) * (8 + 8) +
          chunks * N * 32;
   }
   return b + 64 * 16 * 64;  // per-buffer allocation granularity

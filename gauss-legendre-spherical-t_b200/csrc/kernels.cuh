@@ -269,8 +269,9 @@ __device__ __forceinline__ void fma_sincos_signed2(float2 th, float q, float2 *s
 // kSfCellsPerCta consecutive cells.  Per (atom, node): one multiply, a sine
 // and cosine (SFU, or the FMA-pipe polynomial for the last slot pairs), two
 // FMAs, in paired FP32 instructions where two slots go together.  FP32 over a
-// tile of <= kSfAtomTile atoms (|k.d| <~ 25 rad), then FP64: the twiddle
-// e^{-ik.c} and the sum over tiles.
+// tile of <= kSfAtomTile atoms (|k.d| <~ 25 rad), then FP64 over tiles.  S
+// is stored cell-relative; its twiddle e^{-ik.c} is applied by the shell-sum
+// kernel as it loads S.
 constexpr int kSfThreads = 128;
 constexpr int kSfMaxNpt = 12;     // radial nodes per thread, at most
 constexpr int kSfCellsPerCta = 2;
@@ -300,8 +301,8 @@ __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restric
                                         const uint32_t *__restrict__ cell_count,
                                         const uint32_t *__restrict__ cell_point, const Grid &g,
                                         const float4 *__restrict__ dirs, const float *__restrict__ kappa,
-                                        const double4 *__restrict__ node64, uint32_t c0,
-                                        uint32_t c1, double2 *__restrict__ S, float4 *s_at, float2 *s_f) {
+                                        uint32_t c0,
+                                        uint32_t c1, float2 *__restrict__ S, float4 *s_at, float2 *s_f) {
   // Slots are handled in pairs (FMUL2/FFMA2); an odd last slot alone.
   constexpr int NP2 = NPT / 2;
   constexpr bool ODD = (NPT & 1) != 0;
@@ -326,8 +327,6 @@ __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restric
   for (uint32_t cell = c0; cell < c1; cell++) {
     const uint32_t cnt = cell_count[cell];
     const uint32_t start = cell_point[cell];
-    const uint32_t ix = cell / (g.ny * g.nz), iy = (cell / g.nz) % g.ny, iz = cell % g.nz;
-    const double cx = cell_centre(ix, g.l), cy = cell_centre(iy, g.l), cz = cell_centre(iz, g.l);
     uint32_t a0 = 0;
     do {
       const uint32_t na = min((uint32_t)kSfAtomTile, cnt - a0);
@@ -370,7 +369,11 @@ __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restric
         }
       }
       // Tile sums to shared memory in the unit's node order, then one thread
-      // per node (coalesced): FP64 twiddle, S store or add.
+      // per node (coalesced): S store or add.  S holds the cell-relative
+      // sums in FP32 (each is an FP32 tile sum already; FP64 storage held no
+      // more information and doubled the bytes written here and read by the
+      // shell sums); the shell-sum kernel applies the twiddle e^{-ik.c} in
+      // FP64 from its per-axis tables as it loads S.
       if (act) {
 #pragma unroll
         for (int k = 0; k < NP2; k++) {
@@ -382,19 +385,13 @@ __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restric
       __syncthreads();
       for (uint32_t m = threadIdx.x; m < nodes; m += kSfThreads) {
         const uint32_t k = u.node_begin + m;
-        const double4 kn = node64[k];
-        double ts, tc;
-        sincos(kn.x * cx + kn.y * cy + kn.z * cz, &ts, &tc);
         const float2 f = s_f[m];
-        const double sr = f.x, si = f.y;
-        // (sr + i si) * (tc - i ts)
-        const double2 v = make_double2(sr * tc + si * ts, si * tc - sr * ts);
-        double2 *dst = S + sr_index(cell, k, g.ncell);
+        float2 *dst = S + sr_index(cell, k, g.ncell);
         if (a0 == 0) {
-          *dst = v;
+          *dst = f;
         } else {
-          const double2 o = *dst;
-          *dst = make_double2(o.x + v.x, o.y + v.y);
+          const float2 o = *dst;
+          *dst = make_float2(o.x + f.x, o.y + f.y);
         }
       }
       a0 += kSfAtomTile;
@@ -402,20 +399,19 @@ __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restric
   }
 }
 
-// node64 and S are offset to the launch's first local node; units index
-// them from there.
+// Units index S by local node.
 __global__ void __launch_bounds__(kSfThreads, 8)
 k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_count,
                     const uint32_t *__restrict__ cell_point, Grid g, const SfUnit *__restrict__ units,
                     const float4 *__restrict__ dirs, const float *__restrict__ kappa,
-                    const double4 *__restrict__ node64, double2 *__restrict__ S) {
+                    float2 *__restrict__ S) {
   __shared__ float4 s_at[kSfAtomTile];
   __shared__ float2 s_f[kSfThreads * kSfMaxNpt];
   const SfUnit u = units[blockIdx.x];
   const uint32_t c0 = blockIdx.y * kSfCellsPerCta;
   const uint32_t c1 = min(g.ncell, c0 + kSfCellsPerCta);
 #define GLST_SF_CASE(n) \
-  case n: sf_unit<n>(u, pk, cell_count, cell_point, g, dirs, kappa, node64, c0, c1, S, s_at, s_f); break;
+  case n: sf_unit<n>(u, pk, cell_count, cell_point, g, dirs, kappa, c0, c1, S, s_at, s_f); break;
   switch (u.npt) {
     GLST_SF_CASE(1) GLST_SF_CASE(2) GLST_SF_CASE(3) GLST_SF_CASE(4) GLST_SF_CASE(5) GLST_SF_CASE(6)
     GLST_SF_CASE(7) GLST_SF_CASE(8) GLST_SF_CASE(9) GLST_SF_CASE(10) GLST_SF_CASE(11) GLST_SF_CASE(12)
@@ -436,7 +432,7 @@ constexpr int kSatThreadsOne = 1024;  // one node per CTA (large grids): more wa
 constexpr int kSatLoadBatch = 4;
 
 struct SatArgs {
-  const double2 *S;
+  const float2 *S;               // cell-relative structure factors
   const double4 *node64;        // (kx, ky, kz, w) FP64
   const uint32_t *node_radii;   // r_in | r_out << 16
   uint32_t K;                   // nodes handled by this launch
@@ -500,6 +496,22 @@ k_shell_sums(Grid g, SatArgs a) {
   const uint32_t k = k0 + j;         // node within the launch (node tables)
   const uint32_t ks = a.kbase + k;   // node within S and R
   const bool jv = k < a.K;
+  // The S loads run as a flat sequence of batches (line l, z from z0) of
+  // kSatLoadBatch cells each; the first is issued before the twiddle tables,
+  // whose node loads and FP64 sincos it overlaps (water10k shell sums 0.441
+  // vs 0.450 ms; one batch in flight ahead of the one summed, 0.462 ms at a
+  // batch of 2 and spilling at 4).
+  const uint32_t nlines = g.nx * g.ny;
+  const double2 zero = make_double2(0.0, 0.0);
+  auto fetch = [&](float2 *v, uint32_t l, uint32_t z0) {
+#pragma unroll
+    for (int u = 0; u < kSatLoadBatch; u++)
+      v[u] = (jv && l < nlines && z0 + u < g.nz) ? __ldg(a.S + sr_index(l * g.nz + z0 + u, ks, C))
+                                                   : make_float2(0.f, 0.f);
+  };
+  float2 v[kSatLoadBatch];
+  uint32_t l = first, z0 = 0;
+  fetch(v, l, z0);
   // twiddle tables: e^{i k_a (i + 1/2) l} per node and axis
   for (uint32_t t = threadIdx.x; t < nb * naxis; t += blockDim.x) {
     const uint32_t jj = t / naxis, r = t - jj * naxis;
@@ -520,29 +532,35 @@ k_shell_sums(Grid g, SatArgs a) {
   if (a.xyz_table)
     for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) s_xyz[c] = coords(c);
   double2 *row = s_sat + (size_t)j * a.stride;
-  // S[c][k0 + j] -> row j, summed along z on the way in (the z prefix pass
-  // without its own shared-memory round trip); kSatLoadBatch loads of a line
-  // in flight per thread (one at a time left every thread waiting out a DRAM
-  // round trip per cell)
+  const double2 *twx = s_tw + (size_t)j * naxis, *twy = twx + g.nx, *twz = twy + g.ny;
+  __syncthreads();  // twiddle tables
+  // S[c][k0 + j] -> row j: the cell-relative structure factors times
+  // e^{-ik.c} (the per-axis tables), summed along z on the way in (the z
+  // prefix pass without its own shared-memory round trip)
   {
-    const double2 zero = make_double2(0.0, 0.0);
-    for (uint32_t l = first; l < g.nx * g.ny; l += step) {
+    double2 acc = zero, txy = zero;
+    while (l < nlines) {
+      uint32_t ln = l, zn = z0 + kSatLoadBatch;
+      if (zn >= g.nz) { ln = l + step; zn = 0; }
+      if (z0 == 0) {
+        const uint32_t lx = l / g.ny;
+        txy = cmul(twx[lx], twy[l - lx * g.ny]);  // e^{+i(kx cx + ky cy)}
+        acc = zero;
+      }
       const uint32_t base = l * g.nz;
-      double2 acc = zero;
-      for (uint32_t z0 = 0; z0 < g.nz; z0 += kSatLoadBatch) {
-        double2 v[kSatLoadBatch];
 #pragma unroll
-        for (int u = 0; u < kSatLoadBatch; u++)
-          v[u] = (jv && z0 + u < g.nz) ? __ldg(a.S + sr_index(base + z0 + u, ks, C)) : zero;
-#pragma unroll
-        for (int u = 0; u < kSatLoadBatch; u++) {
-          if (z0 + u < g.nz) {
-            acc.x += v[u].x;
-            acc.y += v[u].y;
-            row[base + z0 + u] = acc;
-          }
+      for (int u = 0; u < kSatLoadBatch; u++) {
+        if (z0 + u < g.nz) {
+          const double2 t = cmul(txy, twz[z0 + u]);  // e^{+ik.c}
+          const double vx = v[u].x, vy = v[u].y;
+          acc.x += vx * t.x + vy * t.y;  // v * conj(t)
+          acc.y += vy * t.x - vx * t.y;
+          row[base + z0 + u] = acc;
         }
       }
+      fetch(v, ln, zn);
+      l = ln;
+      z0 = zn;
     }
   }
   __syncthreads();
@@ -569,7 +587,6 @@ k_shell_sums(Grid g, SatArgs a) {
   const uint32_t radii = a.node_radii[k];
   const uint32_t r_out = radii >> 16, r_in = radii & 0xffffu;
   const double w = a.node64[k].w;
-  const double2 *twx = s_tw + (size_t)j * naxis, *twy = twx + g.nx, *twz = twy + g.ny;
   for (uint32_t c = first; c < C; c += step) {
     const uint32_t xyz = a.xyz_table ? s_xyz[c] : coords(c);
     const uint32_t x = xyz & 1023u, y = (xyz >> 10) & 1023u, z = xyz >> 20;
