@@ -739,7 +739,11 @@ static glst_status compute_all(glst_handle *h, const double *rx, const double *r
   // shell sums of one range (shared-memory bound) could overlap the SFU-bound
   // kernels of the next.  Measured on B200 it does not: the structure-factor
   // kernel fills every SM's register file, so the other stream's blocks only
-  // start as it drains.  kFarStages is therefore 1 (the plain sequence).
+  // start as it drains.  Nor does putting every stage's structure factors on
+  // this stream and each stage's shell sums and gather behind them on a
+  // highest-priority stream (water10k 3.27 / 3.35 / 3.42 ms per solve at 2 /
+  // 4 / 8 stages against 3.14 ms).  kFarStages is therefore 1 (the plain
+  // sequence).
   if (h->K && h->plan.natom && !h->ranges.empty()) {
     CUDA_TRY(cudaStreamWaitEvent(h->far2, h->ev_fork, 0));
     for (size_t r = 0; r < h->ranges.size(); r++) {
