@@ -628,12 +628,15 @@ struct LrChunk {
 // zero node -- stored as float4 (R'x_r, R'x_r+1, R'y_r, R'y_r+1) so that the
 // paired FP32 instructions (FMUL2/FFMA2) do two nodes at once:
 //   EA += c R'x,  EB += s R'y,  G += kappa (c R'y + s R'x),   e = EA - EB.
-// One pair in kLrGroup takes its sine and cosine from the FMA-pipe
+// One pair in kLrPolyStride takes its sine and cosine from the FMA-pipe
 // polynomial, interleaved with the SFU pairs of its group (the FMA pipe
 // already carries ~7 FP32 operations per node, so only a small share pays):
 // water10k 1.57 ms with none, 1.51 ms with 1 in 7, 1.53 with 1 in 5, 1.66
 // with 1 in 3; a separate polynomial loop after the SFU loop (20-40 %)
-// measured 1.63-1.87 ms.
+// measured 1.63-1.87 ms.  The radial scales load as float4 quads (two
+// pairs), so groups are even: 14 pairs with 2 on the polynomial, 1.462 ms
+// against 1.482 ms with one scale load per pair (groups of 6 / 8 / 12 / 16
+// pairs with 1 / 1 / 2 / 2 on the polynomial: 1.503 / 1.483 / 1.476 / 1.498).
 // The cell slots of a tile are kLrfSlotPad float4 apart beyond the tile so
 // that the up to four addresses a warp reads fall in different shared-memory
 // banks (32.9 M bank conflicts per launch without the pad, 0.25 M with).
@@ -643,7 +646,9 @@ constexpr int kLrfTileNodes = 2 * kLrfTilePairs;
 constexpr int kLrfSlotPad = 2;
 constexpr int kLrfSlot = kLrfTilePairs + kLrfSlotPad;
 constexpr int kLrfPerThread = (kLrfCells * kLrfTilePairs) / kLrThreads;
-constexpr int kLrGroup = 7;  // node pairs per group, the last one on the FMA pipe
+constexpr int kLrGroup = 14;      // node pairs per group (even: radial scales load as quads)
+constexpr int kLrPolyStride = 7;  // pair q of a group is on the FMA pipe when q % 7 == 6
+static_assert(kLrGroup % 2 == 0, "groups are whole radial-scale quads");
 
 __device__ __forceinline__ uint32_t cell_of_atom(const uint32_t *__restrict__ cell_point, uint32_t ncell,
                                                  uint32_t p) {
@@ -663,7 +668,7 @@ k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ ce
                   const float *__restrict__ kappa, const float2 *__restrict__ R, uint32_t natom,
                   double4 *__restrict__ part) {
   __shared__ float4 s_n[2][kLrfCells * kLrfSlot];
-  __shared__ float2 s_kappa2[kLrfTilePairs];
+  __shared__ float4 s_kappa4[kLrfTilePairs / 2];
   __shared__ uint32_t s_range[2];
   const uint32_t a0 = blockIdx.x * kLrThreads;
   const uint32_t p = a0 + threadIdx.x;
@@ -673,9 +678,12 @@ k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ ce
   const uint32_t npr = (nr + 1) >> 1;                                   // pairs per direction
   const uint32_t dirs_per_tile = max(1u, (uint32_t)kLrfTilePairs / npr);  // npr <= kLrfTilePairs (host check)
   const uint32_t ntiles = (ch.n_dir + dirs_per_tile - 1) / dirs_per_tile;
-  for (uint32_t t = threadIdx.x; t < npr; t += kLrThreads) {
-    const uint32_t r = 2 * t;
-    s_kappa2[t] = make_float2(kappa[ch.kappa_begin + r], r + 1 < nr ? kappa[ch.kappa_begin + r + 1] : 0.f);
+  // radial scales of pairs (2t, 2t+1): kappa_{4t .. 4t+3}, 0 beyond the last
+  for (uint32_t t = threadIdx.x; 2 * t < npr; t += kLrThreads) {
+    float kq[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) kq[i] = 4 * t + i < nr ? kappa[ch.kappa_begin + 4 * t + i] : 0.f;
+    s_kappa4[t] = make_float4(kq[0], kq[1], kq[2], kq[3]);
   }
   const uint32_t last = min(a0 + kLrThreads, natom) - 1;
   if (threadIdx.x == 0) s_range[0] = cell_of_atom(cell_point, ncell, a0);
@@ -731,37 +739,13 @@ k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ ce
           const float2 u2 = bcast(u);
           float2 EA = make_float2(0.f, 0.f), EB = make_float2(0.f, 0.f), G = make_float2(0.f, 0.f);
           const float4 *nn = cb + d * npr;
-          // groups of kLrGroup pairs: the last of each group takes its sine
-          // and cosine from the FMA-pipe polynomial, interleaved with the SFU
-          // pairs of the same group; the remaining pairs use the SFU
-          uint32_t k = 0;
-          for (; k + kLrGroup <= npr; k += kLrGroup) {
-#pragma unroll
-            for (int q = 0; q < kLrGroup; q++) {
-              const float4 v = nn[k + q];
-              const float2 kp = s_kappa2[k + q];
-              const float2 th = __fmul2_rn(kp, u2);
-              float2 C, Sn, RX = make_float2(v.x, v.y), RY = make_float2(v.z, v.w);
-              if (q == kLrGroup - 1) {
-                float2 sg;
-                fma_sincos_signed2(th, 1.0f, &Sn, &C, &sg);  // sg = (+-1, +-1)
-                RX = __fmul2_rn(RX, sg);
-                RY = __fmul2_rn(RY, sg);
-              } else {
-                float s0, c0, s1, c1;
-                sfu_sincos(th.x, &s0, &c0);
-                sfu_sincos(th.y, &s1, &c1);
-                C = make_float2(c0, c1);
-                Sn = make_float2(s0, s1);
-              }
-              EA = __ffma2_rn(C, RX, EA);
-              EB = __ffma2_rn(Sn, RY, EB);
-              G = __ffma2_rn(kp, __ffma2_rn(C, RY, __fmul2_rn(Sn, RX)), G);
-            }
-          }
-          for (; k < npr; k++) {
-            const float4 v = nn[k];
-            const float2 kp = s_kappa2[k];
+          // Groups of kLrGroup pairs: pair q with q % kLrPolyStride ==
+          // kLrPolyStride - 1 takes its sine and cosine from the FMA-pipe
+          // polynomial, interleaved with the SFU pairs of its group; the
+          // remaining pairs use the SFU.  The radial scales of two pairs come
+          // in one 16-byte load (the R' pair and the scales were two shared
+          // loads per node pair in the MIO queue beside four MUFU operations).
+          auto sfu_pair = [&](const float4 &v, float2 kp) {
             const float2 th = __fmul2_rn(kp, u2);
             float s0, c0, s1, c1;
             sfu_sincos(th.x, &s0, &c0);
@@ -771,6 +755,37 @@ k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ ce
             EA = __ffma2_rn(C, RX, EA);
             EB = __ffma2_rn(Sn, RY, EB);
             G = __ffma2_rn(kp, __ffma2_rn(C, RY, __fmul2_rn(Sn, RX)), G);
+          };
+          uint32_t k = 0;  // even throughout
+          for (; k + kLrGroup <= npr; k += kLrGroup) {
+            float4 kq;
+#pragma unroll
+            for (int q = 0; q < kLrGroup; q++) {
+              if ((q & 1) == 0) kq = s_kappa4[(k + q) >> 1];
+              const float2 kp = (q & 1) ? make_float2(kq.z, kq.w) : make_float2(kq.x, kq.y);
+              const float4 v = nn[k + q];
+              if (q % kLrPolyStride == kLrPolyStride - 1) {
+                const float2 th = __fmul2_rn(kp, u2);
+                float2 C, Sn, sg;
+                fma_sincos_signed2(th, 1.0f, &Sn, &C, &sg);  // sg = (+-1, +-1)
+                const float2 RX = __fmul2_rn(make_float2(v.x, v.y), sg);
+                const float2 RY = __fmul2_rn(make_float2(v.z, v.w), sg);
+                EA = __ffma2_rn(C, RX, EA);
+                EB = __ffma2_rn(Sn, RY, EB);
+                G = __ffma2_rn(kp, __ffma2_rn(C, RY, __fmul2_rn(Sn, RX)), G);
+              } else {
+                sfu_pair(v, kp);
+              }
+            }
+          }
+          for (; k + 2 <= npr; k += 2) {
+            const float4 kq = s_kappa4[k >> 1];
+            sfu_pair(nn[k], make_float2(kq.x, kq.y));
+            sfu_pair(nn[k + 1], make_float2(kq.z, kq.w));
+          }
+          if (k < npr) {
+            const float4 kq = s_kappa4[k >> 1];
+            sfu_pair(nn[k], make_float2(kq.x, kq.y));
           }
           const float e = (EA.x + EA.y) - (EB.x + EB.y), gsum = G.x + G.y;
           te += e;
