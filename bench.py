@@ -424,6 +424,19 @@ def run_ours(args, world, rank, local, dist):
         "pairs_per_launch": pairs,
         "fp32_fma_peak_per_s": fma_peak,
     }
+    # The same kernel's algorithmic FP32 work against the measured FMA-pipe
+    # peak: per (atom, node) the phase kappa*u and the accumulation (five
+    # operations in the gather: c R'x, s R'y, s R'x, c R'y, kappa*(...); two
+    # in the structure factors), per (atom, direction) u = s.d (three).  The
+    # FMA-pipe sine/cosine share is not counted: it stands in for MUFU work.
+    n_dir = sum(inf.group_nodes[i] / (inf.group_gl_degree[i] // 2) for i in range(inf.ngroup))
+    ops_pair = 6.0 if dom == "long_range" else 3.0
+    fma_ops = float(n) * (ops_pair * K + 3.0 * n_dir)
+    fma_ach = fma_ops / (phases[dom] * 1e-3)
+    roofline["fma"] = {"achieved": fma_ach / 1e9, "peak": fma_peak / 1e9, "unit": "G FP32 ops/s",
+                       "frac": fma_ach / fma_peak, "ops_per_launch": fma_ops,
+                       "peak_source": "measured on this GPU by glst_measure_pipe_peaks (FP32 FMA loop)",
+                       "reading": "not the bound: the FMA pipe carries this plus part of the sin/cos"}
     # The same kernel against the HBM roofline (MEASURED_PEAKS.json): its
     # algorithmic bytes are the cross-cell operand it streams once (R read
     # for the gather, S written for the structure factors: C x K float2).
