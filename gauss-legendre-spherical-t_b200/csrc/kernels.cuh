@@ -294,6 +294,9 @@ struct SfUnit {
 // (npt 11 / 9 / 10 in its three groups): SF 1.47 ms with no pairs, 1.31 ms
 // with (npt - 1) / 4 (2/2/2), 1.25 ms with (npt - 3) / 4 (2/1/1), 1.28 ms
 // with one pair everywhere, 1.29 ms with (npt - 3) / 3 (2/2/2 + ...).
+// Re-measured with S stored cell-relative in FP32 (no FP64 epilogue): 1.10 ms
+// with (npt - 3) / 4, 1.16 with (npt - 5) / 4, 1.17 with npt / 4, 1.19 with
+// (npt - 1) / 4, 1.30 with (npt + 1) / 4.
 __host__ __device__ constexpr int sf_poly_pairs(int npt) { return (npt - 3) / 4; }
 
 template <int NPT>
