@@ -418,7 +418,7 @@ def run_ours(args, world, rank, local, dist):
         "bound": "sfu", "kernel": dom, "achieved": achieved_sfu / 1e9, "peak": sfu_peak / 1e9,
         "unit": "G sincos-results/s", "frac": achieved_sfu / sfu_peak,
         "peak_source": "measured on this GPU by glst_measure_pipe_peaks (MUFU sin+cos loop)",
-        "traffic": 3.181e8 if dom == "long_range" else 2.198e8,
+        "traffic": 3.208e8 if dom == "long_range" else 2.196e8,
         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of this "
                           "kernel on this workload (profiles/water10k_solve_kernels.md)",
         "pairs_per_launch": pairs,
