@@ -506,11 +506,11 @@ k_shell_sums(Grid g, SatArgs a) {
   // batch of 2 and spilling at 4).
   const uint32_t nlines = g.nx * g.ny;
   const double2 zero = make_double2(0.0, 0.0);
-  auto fetch = [&](float2 *v, uint32_t l, uint32_t z0) {
+  auto fetch = [&](float2 *dst, uint32_t line, uint32_t zb) {
 #pragma unroll
     for (int u = 0; u < kSatLoadBatch; u++)
-      v[u] = (jv && l < nlines && z0 + u < g.nz) ? __ldg(a.S + sr_index(l * g.nz + z0 + u, ks, C))
-                                                   : make_float2(0.f, 0.f);
+      dst[u] = (jv && line < nlines && zb + u < g.nz) ? __ldg(a.S + sr_index(line * g.nz + zb + u, ks, C))
+                                                      : make_float2(0.f, 0.f);
   };
   float2 v[kSatLoadBatch];
   uint32_t l = first, z0 = 0;
