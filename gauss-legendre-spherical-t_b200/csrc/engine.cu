@@ -656,10 +656,13 @@ static glst_status shell_range(glst_handle *h, uint32_t kb, uint32_t ke, cudaStr
   if (ke <= kb || !h->plan.natom) return GLST_OK;
   uint32_t lg = 0;
   while ((1u << lg) < h->sat_nb) lg++;
+  // the cell-coordinate table serves the several-nodes form only (the
+  // one-node form steps its cells' coordinates)
+  const bool table = h->sat_xyz && h->sat_nb > 1;
   dev::SatArgs a{h->S, h->node64 + h->k_begin + kb, h->node_radii + h->k_begin + kb, ke - kb, kb,
-                 h->sat_nb, lg, h->sat_xyz ? 1u : 0u, h->sat_stride, h->R};
+                 h->sat_nb, lg, table ? 1u : 0u, h->sat_stride, h->R};
   const uint32_t nblk = (ke - kb + h->sat_nb - 1) / h->sat_nb;
-  const size_t smem = h->sat_per_node * h->sat_nb + (h->sat_xyz ? (((size_t)h->plan.ncell * 4 + 15) & ~size_t(15)) : 0);
+  const size_t smem = h->sat_per_node * h->sat_nb + (table ? (((size_t)h->plan.ncell * 4 + 15) & ~size_t(15)) : 0);
   // several nodes per CTA: 512 threads, 3 CTAs per SM; one node per CTA
   // (large grids, one CTA fills the shared memory): 1024 threads
   if (h->sat_nb == 1)

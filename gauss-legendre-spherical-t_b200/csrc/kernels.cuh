@@ -475,8 +475,9 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 }
 
 // Dynamic shared memory: nb rows of `stride` complex (the SAT), the twiddle
-// tables nb x (nx + ny + nz) complex, then (when it fits) the cell coordinates
-// (ncell x u32, x | y << 10 | z << 20).  nb is a power of two <= 32: lane l of a warp works
+// tables nb x (nx + ny + nz) complex, then, in the several-nodes form
+// (kMinBlocks > 1, small grids) when it fits, the cell coordinates (ncell x
+// u32, x | y << 10 | z << 20).  nb is a power of two <= 32: lane l of a warp works
 // on node l % nb of the CTA and on the (l / nb)-th of the 32 / nb cells or
 // lines the warp takes per step, so the per-node values (radii, weight,
 // twiddle rows) stay in registers and the S loads and R stores of a warp are
@@ -532,7 +533,7 @@ k_shell_sums(Grid g, SatArgs a) {
     const uint32_t y = rem / g.nz, z = rem - y * g.nz;
     return x | (y << 10) | (z << 20);
   };
-  if (a.xyz_table)
+  if (kMinBlocks > 1 && a.xyz_table)
     for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) s_xyz[c] = coords(c);
   double2 *row = s_sat + (size_t)j * a.stride;
   const double2 *twx = s_tw + (size_t)j * naxis, *twy = twx + g.nx, *twz = twy + g.ny;
@@ -590,14 +591,38 @@ k_shell_sums(Grid g, SatArgs a) {
   const uint32_t radii = a.node_radii[k];
   const uint32_t r_out = radii >> 16, r_in = radii & 0xffffu;
   const double w = a.node64[k].w;
-  for (uint32_t c = first; c < C; c += step) {
-    const uint32_t xyz = a.xyz_table ? s_xyz[c] : coords(c);
-    const uint32_t x = xyz & 1023u, y = (xyz >> 10) & 1023u, z = xyz >> 20;
-    const double2 o = cube_sum(row, x, y, z, r_out, g);
-    const double2 i = cube_sum(row, x, y, z, r_in, g);
-    const double2 sh = make_double2((o.x - i.x) * w, (o.y - i.y) * w);
-    const double2 r = cmul(cmul(sh, twx[x]), cmul(twy[y], twz[z]));
-    a.R[sr_index(c, ks, C)] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
+  // The thread's cells c = first + i * step.  Small grids (several nodes per
+  // CTA) look their coordinates up in the CTA's table.  Large grids (one node
+  // per CTA) step them with carries: there the table cost every CTA two
+  // divisions per cell of the grid (water333k shell sums 34.8 ms with it,
+  // 27.9 ms stepping); on small grids stepping measured slower (water10k
+  // 0.43 against 0.42 ms).
+  if constexpr (kMinBlocks > 1) {
+    for (uint32_t c = first; c < C; c += step) {
+      const uint32_t xyz = a.xyz_table ? s_xyz[c] : coords(c);
+      const uint32_t x = xyz & 1023u, y = (xyz >> 10) & 1023u, z = xyz >> 20;
+      const double2 o = cube_sum(row, x, y, z, r_out, g);
+      const double2 i = cube_sum(row, x, y, z, r_in, g);
+      const double2 sh = make_double2((o.x - i.x) * w, (o.y - i.y) * w);
+      const double2 r = cmul(cmul(sh, twx[x]), cmul(twy[y], twz[z]));
+      a.R[sr_index(c, ks, C)] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
+    }
+  } else {
+    const uint32_t syz = g.ny * g.nz;
+    const uint32_t sx = step / syz, sy = (step - sx * syz) / g.nz, sz = step - sx * syz - sy * g.nz;
+    uint32_t x = first / syz, y = (first - x * syz) / g.nz, z = first - x * syz - y * g.nz;
+    for (uint32_t c = first; c < C; c += step) {
+      const double2 o = cube_sum(row, x, y, z, r_out, g);
+      const double2 i = cube_sum(row, x, y, z, r_in, g);
+      const double2 sh = make_double2((o.x - i.x) * w, (o.y - i.y) * w);
+      const double2 r = cmul(cmul(sh, twx[x]), cmul(twy[y], twz[z]));
+      a.R[sr_index(c, ks, C)] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
+      z += sz;  // sz < nz and sy < ny: one carry at most per axis
+      if (z >= g.nz) { z -= g.nz; y++; }
+      y += sy;
+      if (y >= g.ny) { y -= g.ny; x++; }
+      x += sx;
+    }
   }
 }
 
