@@ -40,7 +40,7 @@ def _rank(rank, world, port, out):
 
 def test_weak_scaling_uses_max_over_ranks():
     world = 2
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()  # no fork of a threaded test process
     out = mgr.dict()
     mp.spawn(_rank, args=(world, _free_port(), out), nprocs=world, join=True)
     for r in range(world):
@@ -80,7 +80,7 @@ def test_node_shards_sum_over_gloo(store, case):
     from oracle import oracle, planner
     from test_golden import load_case
     world = 2
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()  # no fork of a threaded test process
     out = mgr.dict()
     mp.spawn(_shard_rank, args=(world, _free_port(), case, out), nprocs=world, join=True)
     d, (x, y, z, q), box = load_case(case, "double")
