@@ -54,6 +54,20 @@ def test_oracle_reproduces_reference_double_path(store, case):
     assert rep["energy_rel"] < 1e-13, rep
 
 
+@pytest.mark.slow
+@pytest.mark.parametrize("case", ["water10k", "water10k_next"])
+def test_oracle_reproduces_reference_double_path_large(store, case):
+    """10,000 waters at the default order (K = 100,532) and the next order
+    (tol / 10, K = 192,478): a full FP64 solve each, ~20-40 s on 8 cores."""
+    d, (x, y, z, q), box = load_case(case, "double")
+    p = planner.make_plan(len(x), float(d["tol"]), box, float(d["rcut"]), store)
+    assert p.K == int(d["K"]) and p.n == tuple(int(v) for v in d["ncell"])
+    got = oracle.glst(x, y, z, q, p)
+    rep = oracle.error_report(got, (d["fx"], d["fy"], d["fz"], d["en"]))
+    assert rep["force_rms_rel"] < 1e-13, rep
+    assert rep["energy_rel"] < 1e-13, rep
+
+
 @pytest.mark.parametrize("case", SMALL + ["water10k"])
 @pytest.mark.parametrize("ct", ["double", "float"])
 def test_oracle_assignment_bitexact_with_reference(store, case, ct):
