@@ -13,7 +13,7 @@ system (independent systems, no collective on the data path): weak scaling,
 value = all ranks' atoms / max-over-ranks time.
 --impl reference times the FP64 CPU restatement of the reference's GLST sum
 (the reference ships no CPU implementation; its own code is CUDA) on the
-host's cores, on a node subset of the same workload, extrapolated by K.
+host's cores: every timed step one complete solve of the same workload.
 """
 import argparse
 import json
@@ -120,51 +120,53 @@ def dist_setup(args):
     return world, rank, local, pg
 
 
-def cpu_baseline_run(sysd, K_sample_div=32):
-    """FP64 oracle on the host: full near field + a node subset of the far
-    field, extrapolated linearly in the number of nodes."""
+def cpu_baseline_run(sysd, full=True, K_sample_div=32):
+    """FP64 oracle on the host cores: one complete solve of the workload
+    (assignment, structure factors, shell sums and gather over all K nodes,
+    near field), timed by the wall clock.  full=False solves the near field
+    and 1/K_sample_div of the nodes only (a warm-up that touches every code
+    path in a fraction of the time)."""
     from oracle import oracle, planner
     g = __graft_entry__.load_package()
     store = planner.TDesignStore(g.TDESIGN_STORE)
     x, y, z, q = sysd["x"], sysd["y"], sysd["z"], sysd["q"]
     p = planner.make_plan(len(x), sysd["tol"], sysd["box"], sysd["rcut"], store)
-    ks = max(1, p.K // K_sample_div)
+    k1 = p.K if full else max(1, p.K // K_sample_div)
     t0 = time.perf_counter()
-    oracle.glst(x, y, z, q, p, far=False, sr=True)
-    t_sr = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    oracle.glst(x, y, z, q, p, k0=0, k1=ks, far=True, sr=False)
-    t_far = time.perf_counter() - t0
-    t_est = t_sr + t_far * (p.K / ks)
-    return dict(seconds_per_solve=t_est, cores=oracle.num_threads(), K=p.K, K_sample=ks,
-                t_near=t_sr, t_far_sample=t_far)
+    oracle.glst(x, y, z, q, p, k0=0, k1=k1)
+    t = time.perf_counter() - t0
+    return dict(seconds_per_solve=t, cores=oracle.num_threads(), K=p.K, K_used=k1)
 
 
 def run_reference(args, world, rank):
+    """The reference's GLST sum on the host cores (the reference ships no CPU
+    path; this is the FP64 oracle, a kernel-by-kernel restatement of its
+    double path, OpenMP over all cores).  Warm-up steps solve the near field
+    and 1/32 of the nodes; every timed step is one complete solve."""
     __graft_entry__.load_package()
     from glst_b200 import systems
     if rank != 0:
         return
     sysd = systems.config_system(args.workload, seed=0)
     n = len(sysd["x"])
+    for _ in range(args.warmup):
+        cpu_baseline_run(sysd, full=False)
     times = []
     info = None
-    for it in range(args.warmup + args.steps):
-        r = cpu_baseline_run(sysd)
-        if it >= args.warmup:
-            times.append(r["seconds_per_solve"])
-        info = r
+    for _ in range(args.steps):
+        info = cpu_baseline_run(sysd, full=True)
+        times.append(info["seconds_per_solve"])
     sec = statistics.mean(times)
     val = n / sec
+    sample = "every timed step one complete FP64 solve of the workload (all %d atoms, all %d nodes), wall clock" % (
+        n, info["K"])
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded TIP3P-like water)",
-        "config": {"workload": args.workload, "atoms": n, "nodes": info["K"],
-                   "sample": "all atoms, near field in full, far field on %d of %d nodes, extrapolated in K"
-                             % (info["K_sample"], info["K"])},
-        "cpu_baseline": {"value": val, "unit": UNIT, "cores": info["cores"], "kind": "port",
-                         "sample": "node subset %d/%d, linear in K" % (info["K_sample"], info["K"])},
+        "config": {"workload": args.workload, "atoms": n, "nodes": info["K"], "sample": sample,
+                   "warmup_steps": "near field + 1/32 of the nodes"},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": info["cores"], "kind": "port", "sample": sample},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -185,48 +187,81 @@ def weak_throughput(local_ms, local_atoms, dist=None, device=None):
     return local_ms, world * local_atoms / (local_ms * 1e-3)
 
 
-def run_batch(g, torch, dev, stream, n_steps=4, n_sys=256, seed=0):
+def run_batch(g, torch, dev, stream, sfu_peak, n_steps=4, n_sys=256, seed=0):
     """256 independent water boxes of uneven size (300-30,000 atoms, two
     cubature orders): one captured graph over all systems vs the same systems
-    solved one after another (one launch sequence each)."""
+    solved one after another (one launch sequence each).  Also: the MUFU
+    floor of the pass (sum over systems of N x K x 4 sin/cos results -- two
+    for the structure factors, two for the gather -- at the measured MUFU
+    peak), and the same comparison per system-size class."""
     from glst_b200 import systems
     sy = systems.batch_uneven(n_sys, seed=seed)
-    ins = [torch.tensor(np.concatenate([s[k] for s in sy]), dtype=torch.float64, device=dev)
-           for k in ("x", "y", "z", "q")]
-    n = ins[0].numel()
-    outs = [torch.empty(n, dtype=torch.float64, device=dev) for _ in range(4)]
-    t0 = time.perf_counter()
-    b = g.GlstBatch(sy, nstreams=16)
-    t_create = time.perf_counter() - t0
-    res = {}
-    for mode, plain in (("batched", False), ("plain", True)):
-        for _ in range(2):
-            b.compute(*ins, *outs, plain=plain, stream=stream)
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(n_steps):
-            b.compute(*ins, *outs, plain=plain, stream=stream)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / n_steps
-        res[mode] = {"ms_per_step": ms, "value": n / (ms * 1e-3)}
-    b.close()
-    del ins, outs
-    torch.cuda.empty_cache()
+    infos = [g.plan(s["natom"], s["tol"], s["box"], s["rcut"], with_nodes=False)[0] for s in sy]
+    Ks = [inf.num_nodes if inf.has_far_field else 0 for inf in infos]
+
+    def floor_ms(idx):
+        return sum(4.0 * sy[i]["natom"] * Ks[i] for i in idx) / sfu_peak * 1e3
+
+    def timed(idx, steps):
+        sub = [sy[i] for i in idx]
+        ins = [torch.tensor(np.concatenate([s[k] for s in sub]), dtype=torch.float64, device=dev)
+               for k in ("x", "y", "z", "q")]
+        n = ins[0].numel()
+        outs = [torch.empty(n, dtype=torch.float64, device=dev) for _ in range(4)]
+        t0 = time.perf_counter()
+        b = g.GlstBatch(sub, nstreams=16)
+        t_create = time.perf_counter() - t0
+        res = {}
+        for mode, plain in (("batched", False), ("plain", True)):
+            for _ in range(2):
+                b.compute(*ins, *outs, plain=plain, stream=stream)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                b.compute(*ins, *outs, plain=plain, stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            res[mode] = {"ms_per_step": ms, "value": n / (ms * 1e-3)}
+        b.close()
+        del ins, outs
+        torch.cuda.empty_cache()
+        return n, res, t_create
+
+    all_idx = list(range(len(sy)))
+    n, res, t_create = timed(all_idx, n_steps)
+    fl = floor_ms(all_idx)
     out = {"workload": "%d uneven water boxes, %d atoms (300-30,000 each), 2 cubature orders" % (n_sys, n),
            "unit": UNIT, "batched": res["batched"], "plain": res["plain"],
            "ratio": res["plain"]["ms_per_step"] / res["batched"]["ms_per_step"],
+           "floor_ms": fl, "batched_over_floor": res["batched"]["ms_per_step"] / fl,
+           "plain_over_floor": res["plain"]["ms_per_step"] / fl,
+           "floor_definition": "sum of N x K x 4 sin/cos results / measured MUFU peak (%.3g/s)" % sfu_peak,
            "create_s": t_create, "steps": n_steps}
+    classes = {"small (< 3,000 atoms)": [i for i in all_idx if sy[i]["natom"] < 3000],
+               "medium (3,000-19,999 atoms)": [i for i in all_idx if 3000 <= sy[i]["natom"] < 20000],
+               "large (>= 20,000 atoms)": [i for i in all_idx if sy[i]["natom"] >= 20000]}
+    out["by_size"] = {}
+    for name, idx in classes.items():
+        if not idx:
+            continue
+        nc, rc, _ = timed(idx, n_steps)
+        out["by_size"][name] = {"systems": len(idx), "atoms": nc, "floor_ms": floor_ms(idx),
+                                "batched_ms": rc["batched"]["ms_per_step"], "plain_ms": rc["plain"]["ms_per_step"],
+                                "ratio": rc["plain"]["ms_per_step"] / rc["batched"]["ms_per_step"]}
     # The reference library's plain path on the same 256 systems (one solve
-    # after another, calc_ener_force only), recorded on a B200 with the
-    # reference harness into the batch256 golden fixture.
+    # after another, calc_ener_force only), recorded earlier on a B200 with
+    # the reference harness into the batch256 golden fixture: a recorded
+    # figure, not measured in this run.
     gold = os.path.join(ROOT, "tests", "golden", "batch256_double.npz")
     if n_sys == 256 and seed == 0 and os.path.exists(gold):
         ref_ms = float(np.load(gold)["ms_host"].sum())
-        out["reference_plain_recorded"] = {"ms_per_step": ref_ms, "value": n / (ref_ms * 1e-3),
-                                           "batched_ratio": ref_ms / res["batched"]["ms_per_step"]}
+        out["reference_plain_recorded_not_measured_here"] = {
+            "ms_per_step": ref_ms, "value": n / (ref_ms * 1e-3),
+            "batched_ratio": ref_ms / res["batched"]["ms_per_step"],
+            "source": "tests/golden/batch256_double.npz (reference harness, one B200, recorded)"}
     return out
 
 
@@ -474,18 +509,17 @@ def run_ours(args, world, rank, local, dist):
     if rank == 0 and args.reference_log:
         write_reference_log(args.reference_log, args.workload, g, f, inf, sysd, d, stream, dev, torch, iters=20)
     if world == 1 and not args.no_batch:
-        line["batched_vs_plain"] = run_batch(g, torch, dev, stream, n_steps=max(2, args.steps // 5))
+        line["batched_vs_plain"] = run_batch(g, torch, dev, stream, sfu_peak, n_steps=max(2, args.steps // 5))
     if world == 1 and not args.no_serve:
         f.close()
         torch.cuda.empty_cache()
         line["served"] = run_serve(g)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = cpu_baseline_run(sysd)
+        cb = cpu_baseline_run(sysd, full=True)
         line["cpu_baseline"] = {"value": n / cb["seconds_per_solve"], "unit": UNIT, "cores": cb["cores"],
                                 "kind": "port",
-                                "sample": "FP64 oracle: near field in full + far field on %d of %d nodes "
-                                          "(%.1f s), extrapolated linearly in K" % (
-                                              cb["K_sample"], cb["K"], cb["t_near"] + cb["t_far_sample"])}
+                                "sample": "one complete FP64 oracle solve of the workload (%d atoms, %d nodes): "
+                                          "%.1f s wall clock" % (n, cb["K"], cb["seconds_per_solve"])}
     if rank == 0:
         print(json.dumps(line), flush=True)
     f.close()

@@ -51,6 +51,8 @@ class GlstInfo(ctypes.Structure):
         ("group_r_out", ctypes.c_uint32 * 16),
         ("device_bytes", ctypes.c_uint64),
         ("kernels_per_compute", ctypes.c_uint32),
+        ("node_stages", ctypes.c_uint32),
+        ("shell_sums_global", ctypes.c_uint32),
     ]
 
 
@@ -79,6 +81,7 @@ _SIGNATURES = {
     "glst_get_info": (_I, [_P, ctypes.POINTER(GlstInfo)]),
     "glst_get_nodes": (_I, [_P, _P, _P, _P, _P, _P]),
     "glst_check": (_I, [_P, _P]),
+    "glst_get_far_field": (_I, [_P, _P, _P, _P, _P, _P]),
     "glst_plan": (_I, [_U32, _D, _D, _D, _D, _D, _I, ctypes.POINTER(GlstInfo), _P, _P, _P, _P, _P]),
     "glst_max_atoms_per_cell": (_U32, []),
     "glst_measure_pipe_peaks": (_I, [_DP, _DP]),
@@ -317,6 +320,17 @@ class GlstForce:
             _check(self._lib.glst_get_info(self._h, ctypes.byref(inf)))
             self._info = inf
         return self._info
+
+    def far_field(self, stream=None):
+        """(sf, rmt): complex128 arrays [ncell, K] of the last assigned
+        positions, in the reference's layout and definitions (its sf_re_/sf_im_
+        after calc_sf and rmt_sum_re_/rmt_sum_im_ after sum_rmt_sf), nodes in
+        the order of ``nodes()``."""
+        inf = self.info()
+        C, K = inf.ncell_total, inf.num_nodes
+        arrs = [np.empty((C, K)) for _ in range(4)]
+        _check(self._lib.glst_get_far_field(self._h, *[a.ctypes.data for a in arrs], _stream(stream)))
+        return arrs[0] + 1j * arrs[1], arrs[2] + 1j * arrs[3]
 
     def nodes(self):
         K = self.info().num_nodes

@@ -123,6 +123,7 @@ struct glst_handle {
   bool sat_xyz = true;  // shell-sum cell-coordinate table in shared memory
   uint32_t combine_blocks = 1;
   bool computed = false;
+  bool assigned = false;  // packets of some positions are in place (far-field accessor)
   std::vector<DevBuf> bufs;
   struct PendingBuf {
     void **out;
@@ -160,13 +161,26 @@ struct glst_handle {
   // host-visible staging for the end-to-end path
   double *in_host = nullptr;  // device copy of host inputs (4 x natom)
   // streams/events for the near-field fork and the far-field pipeline
-  cudaStream_t side = nullptr, far2 = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_far2 = nullptr;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // Node stages: the far field runs stage by stage (structure factors, shell
+  // sums, gather over a contiguous range of whole directions), so S and R
+  // hold one stage's nodes; a large system needs a fraction of the C x K
+  // operand the whole node set would take.
   struct FarRange {
-    uint32_t kb, ke, c0, c1;  // nodes and long-range chunks of one pipeline stage
+    uint32_t kb, ke, c0, c1;  // nodes and long-range chunks of one stage
     uint32_t u0, u1;          // structure-factor units of the same nodes
   };
   std::vector<FarRange> ranges;
+  uint32_t stage_kmax = 0;    // nodes of the largest stage (S and R hold this many)
+  uint32_t part_rows = 1;     // rows of `part` (chunks of the largest stage)
+  uint32_t part_zero_from = 0;  // rows from here on are zeroed before stage 0
+  // shell sums in global memory (grids whose per-node table does not fit
+  // in shared memory): FP64 tables of a batch of node blocks, twiddles
+  bool gsat = false;
+  uint32_t gsat_nblk = 1;     // node blocks per batch
+  double2 *gsat_T = nullptr;  // gsat_nblk x C x kNodeBlock
+  double2 *gsat_tw = nullptr; // stage_kmax x (nx + ny + nz)
 };
 
 // Buffers of a handle are requested first and then carved out of one
@@ -255,12 +269,10 @@ static void release(glst_handle *h, bool device_idle = false) {
   h->chunk_cap = h->unit_cap = h->part_cap = 0;
   h->bytes = 0;
   if (h->side) cudaStreamDestroy(h->side);
-  if (h->far2) cudaStreamDestroy(h->far2);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
   if (h->ev_join) cudaEventDestroy(h->ev_join);
-  if (h->ev_far2) cudaEventDestroy(h->ev_far2);
-  h->side = h->far2 = nullptr;
-  h->ev_fork = h->ev_join = h->ev_far2 = nullptr;
+  h->side = nullptr;
+  h->ev_fork = h->ev_join = nullptr;
 }
 
 // ---------------------------------------------------------------- tuning
@@ -284,7 +296,17 @@ static Tuning tuned(const Plan &p, uint32_t K) {
   return it == g_tune.end() ? Tuning{} : it->second;
 }
 
-static constexpr uint32_t kFarStages = 1;  // far-field pipeline stages per solve (see below)
+// Bytes of S + R one node stage may hold (default 2 GiB; the environment
+// variable GLST_STAGE_BYTES, read when a handle is set up, overrides it).
+// Systems whose C x K operand is larger run in several stages.
+static uint64_t stage_budget() {
+  uint64_t b = 2ull << 30;
+  if (const char *e = std::getenv("GLST_STAGE_BYTES")) {
+    const unsigned long long x = std::strtoull(e, nullptr, 10);
+    if (x >= (1ull << 20)) b = x;
+  }
+  return b;
+}
 
 static uint32_t pow2_floor(uint32_t v) {
   uint32_t p = 1;
@@ -292,102 +314,144 @@ static uint32_t pow2_floor(uint32_t v) {
   return p;
 }
 
-
-// Long-range chunks: whole directions of one group each, sized so that
-// ncell x chunks is about lr_waves waves of resident CTAs; then this
-// device's share when the system is split over several devices.
+// Node stages and long-range chunks.  First this handle's node range: all
+// nodes, or -- when the system is split over several devices -- a contiguous
+// run of whole directions holding about K / nshards nodes (the reference
+// splits its node list into contiguous per-GPU ranges,
+// src/glst_force.cu:276-293).  Then stages: contiguous runs of whole
+// directions of about equal node count, as many as the S + R budget needs.
+// Then, per stage, long-range chunks (whole directions of one group) sized so
+// that the gather's grid is about lr_waves waves of resident CTAs, and the
+// structure-factor units.
 static glst_status build_chunks(glst_handle *h, bool in_arena = false) {
   const Plan &p = h->plan;
-  const size_t C = p.ncell, K = p.has_far ? p.K() : 0, N = p.natom;
+  const size_t C = p.ncell, Kall = p.has_far ? p.K() : 0, N = p.natom;
   const size_t slots = (size_t)h->nsm * 16;
   const size_t want_chunks = std::max<size_t>(1, ((size_t)h->lr_waves * slots + C - 1) / C);
-  const size_t target_nodes = std::max<size_t>(1, K / want_chunks);
-  std::vector<dev::LrChunk> chunks;
-  for (size_t gi = 0; gi < p.groups.size(); gi++) {
-    const auto &g = p.groups[gi];
-    const uint32_t dpc = (uint32_t)std::max<size_t>(1, target_nodes / g.n_radial);
-    for (uint32_t j0 = 0; j0 < g.n_dir; j0 += dpc) {
-      dev::LrChunk c{};
-      c.n_dir = std::min(dpc, g.n_dir - j0);
-      c.n_rad = g.n_radial;
-      c.node_begin = h->g_node_base[gi] + j0 * g.n_radial;
-      c.dir_begin = h->g_dir_base[gi] + j0;
-      c.kappa_begin = h->g_kappa_base[gi];
-      chunks.push_back(c);
-    }
-  }
-  if (h->nshards > 1) {
-    // This device's share of the nodes: a contiguous run of chunks holding
-    // about K/nshards nodes (the reference splits its node list into
-    // contiguous per-GPU ranges, src/glst_force.cu:276-293).
-    std::vector<dev::LrChunk> mine;
-    uint32_t kb = 0, ke = 0;
-    for (const auto &c : chunks) {
-      const uint64_t mid = (uint64_t)c.node_begin + (uint64_t)c.n_dir * c.n_rad / 2;
-      if (mid * h->nshards / K == h->shard) {
-        if (mine.empty()) kb = c.node_begin;
-        ke = c.node_begin + c.n_dir * c.n_rad;
-        mine.push_back(c);
+  struct Dir {
+    uint32_t gi, j;  // group, direction within the group
+    uint32_t k;      // first node (internal order) of the direction
+  };
+  std::vector<Dir> dirs_all;
+  for (size_t gi = 0; gi < (Kall ? p.groups.size() : 0); gi++)
+    for (uint32_t j = 0; j < p.groups[gi].n_dir; j++)
+      dirs_all.push_back({(uint32_t)gi, j, h->g_node_base[gi] + j * p.groups[gi].n_radial});
+  auto dir_nodes = [&](const Dir &d) { return p.groups[d.gi].n_radial; };
+  // this handle's directions [d0, d1)
+  size_t d0 = 0, d1 = dirs_all.size();
+  if (h->nshards > 1 && Kall) {
+    // shard by provisional chunks of ~K / want_chunks nodes, each assigned to
+    // the shard its middle node falls in
+    const size_t target = std::max<size_t>(1, Kall / want_chunks);
+    bool any = false;
+    size_t i = 0;
+    while (i < dirs_all.size()) {
+      const uint32_t gi = dirs_all[i].gi;
+      const uint32_t dpc = (uint32_t)std::max<size_t>(1, target / p.groups[gi].n_radial);
+      size_t e = i;
+      while (e < dirs_all.size() && dirs_all[e].gi == gi && e - i < dpc) e++;
+      const uint64_t nodes = (uint64_t)(e - i) * p.groups[gi].n_radial;
+      const uint64_t mid = (uint64_t)dirs_all[i].k + nodes / 2;
+      if (mid * h->nshards / Kall == h->shard) {
+        if (!any) d0 = i;
+        d1 = e;
+        any = true;
       }
+      i = e;
     }
-    for (auto &c : mine) c.node_begin -= kb;
-    chunks.swap(mine);
-    h->k_begin = kb;
-    h->K = ke - kb;
+    if (!any) d0 = d1 = 0;
   }
-  if (chunks.size() > 65535) return fail(GLST_ERR_SIZE, "too many long-range chunks");
-  h->nsplit = (uint32_t)chunks.size();
-  // pipeline stages: about kFarStages chunk-aligned node ranges
-  h->ranges.clear();
+  const uint32_t kb = d0 < d1 ? dirs_all[d0].k : 0;
+  const uint32_t ke = d0 < d1 ? dirs_all[d1 - 1].k + dir_nodes(dirs_all[d1 - 1]) : 0;
+  h->k_begin = kb;
+  h->K = ke - kb;
+  const uint64_t K = h->K;
+  // stages
+  const uint64_t kpad_all = (K + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock;
+  uint64_t nst = std::max<uint64_t>(1, (C * kpad_all * 16 + stage_budget() - 1) / stage_budget());
+  nst = std::min<uint64_t>(nst, std::max<size_t>(1, d1 - d0));
+  std::vector<std::pair<size_t, size_t>> stage_dirs;  // [first, last) direction of each stage
   {
-    const uint32_t stages = std::min<uint32_t>(kFarStages, h->nsplit);
-    uint32_t c0 = 0;
-    for (uint32_t s = 0; s < stages && c0 < h->nsplit; s++) {
-      const uint64_t target = (uint64_t)h->K * (s + 1) / stages;  // local node count at the stage end
-      uint32_t c1 = c0 + 1;
-      while (c1 < h->nsplit && chunks[c1].node_begin < target) c1++;
-      if (s + 1 == stages) c1 = h->nsplit;
-      const uint32_t kb = chunks[c0].node_begin;
-      const uint32_t ke = chunks[c1 - 1].node_begin + chunks[c1 - 1].n_dir * chunks[c1 - 1].n_rad;
-      h->ranges.push_back({kb, ke, c0, c1, 0, 0});
-      c0 = c1;
+    size_t i = d0;
+    for (uint64_t st = 0; st < nst && i < d1; st++) {
+      const uint64_t target_end = kb + K * (st + 1) / nst;  // node where this stage should end
+      size_t e = i + 1;
+      while (e < d1 && dirs_all[e].k < target_end) e++;
+      if (st + 1 == nst) e = d1;
+      stage_dirs.push_back({i, e});
+      i = e;
     }
   }
-  // Structure-factor units: per stage, each group's run of directions (its
-  // chunks are contiguous) cut into units of kSfThreads / nb directions, nb
-  // threads per direction of npt <= kSfMaxNpt radial nodes.  Cutting the
-  // group's whole run, not each long-range chunk, keeps the units full.
+  // chunks and units per stage
+  std::vector<dev::LrChunk> chunks;
   std::vector<dev::SfUnit> units;
-  for (auto &rg : h->ranges) {
+  h->ranges.clear();
+  h->stage_kmax = 0;
+  h->part_rows = 1;
+  // A shard cuts its chunks at the whole system's chunk size, so that its
+  // chunks are exactly the whole system's chunks of its node range (the
+  // shards' sum then groups every FP32 partial sum as the unsharded solve).
+  const uint64_t kpad_sys = (Kall + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock;
+  const uint64_t nst_sys = std::max<uint64_t>(1, (C * kpad_sys * 16 + stage_budget() - 1) / stage_budget());
+  for (const auto &sd : stage_dirs) {
+    glst_handle::FarRange rg{};
+    rg.kb = dirs_all[sd.first].k - kb;
+    rg.ke = dirs_all[sd.second - 1].k + dir_nodes(dirs_all[sd.second - 1]) - kb;
+    const size_t target_nodes =
+        std::max<size_t>(1, (h->nshards > 1 ? Kall / nst_sys : rg.ke - rg.kb) / want_chunks);
+    rg.c0 = (uint32_t)chunks.size();
     rg.u0 = (uint32_t)units.size();
-    for (uint32_t ci = rg.c0; ci < rg.c1;) {
-      const auto &c = chunks[ci];
-      uint32_t n_dir = c.n_dir, cj = ci + 1;
-      while (cj < rg.c1 && chunks[cj].kappa_begin == c.kappa_begin && chunks[cj].dir_begin == c.dir_begin + n_dir) {
-        n_dir += chunks[cj].n_dir;
-        cj++;
+    size_t i = sd.first;
+    while (i < sd.second) {
+      // this group's run of directions inside the stage
+      const uint32_t gi = dirs_all[i].gi;
+      const auto &g = p.groups[gi];
+      size_t e = i;
+      while (e < sd.second && dirs_all[e].gi == gi) e++;
+      const uint32_t n_dir = (uint32_t)(e - i), j_first = dirs_all[i].j;
+      const uint32_t dpc = (uint32_t)std::max<size_t>(1, target_nodes / g.n_radial);
+      for (uint32_t j0 = 0; j0 < n_dir; j0 += dpc) {
+        dev::LrChunk c{};
+        c.n_dir = std::min(dpc, n_dir - j0);
+        c.n_rad = g.n_radial;
+        c.node_begin = dirs_all[i].k + j0 * g.n_radial - kb;
+        c.dir_begin = h->g_dir_base[gi] + j_first + j0;
+        c.kappa_begin = h->g_kappa_base[gi];
+        chunks.push_back(c);
       }
-      const uint32_t nb = (c.n_rad + dev::kSfMaxNpt - 1) / dev::kSfMaxNpt;
-      const uint32_t npt = (c.n_rad + nb - 1) / nb;
+      // Structure-factor units: the group's whole run cut into units of
+      // kSfThreads / nb directions, nb threads per direction of npt <=
+      // kSfMaxNpt radial nodes (cutting the whole run, not each chunk, keeps
+      // the units full).
+      const uint32_t nb = (g.n_radial + dev::kSfMaxNpt - 1) / dev::kSfMaxNpt;
+      const uint32_t npt = (g.n_radial + nb - 1) / nb;
       const uint32_t dpu = dev::kSfThreads / nb;
       for (uint32_t j0 = 0; j0 < n_dir; j0 += dpu) {
         dev::SfUnit u{};
-        u.node_begin = c.node_begin + j0 * c.n_rad;
-        u.dir_begin = c.dir_begin + j0;
+        u.node_begin = dirs_all[i].k + j0 * g.n_radial - kb;
+        u.dir_begin = h->g_dir_base[gi] + j_first + j0;
         u.n_dir = std::min(dpu, n_dir - j0);
-        u.n_rad = c.n_rad;
+        u.n_rad = g.n_radial;
         u.nb = nb;
         u.npt = npt;
-        u.kappa_begin = c.kappa_begin;
+        u.kappa_begin = h->g_kappa_base[gi];
         units.push_back(u);
       }
-      ci = cj;
+      i = e;
     }
+    rg.c1 = (uint32_t)chunks.size();
     rg.u1 = (uint32_t)units.size();
+    if (rg.c1 - rg.c0 > 65535) return fail(GLST_ERR_SIZE, "too many long-range chunks in a node stage");
+    h->stage_kmax = std::max(h->stage_kmax, rg.ke - rg.kb);
+    h->part_rows = std::max(h->part_rows, rg.c1 - rg.c0);
+    h->ranges.push_back(rg);
   }
+  // rows a later stage writes beyond what stage 0 writes start at zero
+  h->part_zero_from = h->ranges.empty() ? h->part_rows : h->ranges[0].c1 - h->ranges[0].c0;
+  h->nsplit = (uint32_t)chunks.size();
   h->n_sf_units = (uint32_t)units.size();
   if (units.size() > 0x7FFFFFFFu) return fail(GLST_ERR_SIZE, "too many structure-factor units");
-  const size_t part_rows = std::max<size_t>(1, h->nsplit);
+  const size_t part_rows = h->part_rows;
   if (in_arena) {
     // first build (set-up): carve the tables and partial rows out of the
     // handle's single allocation; uploaded once it is committed.  Separate
@@ -471,10 +535,8 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
   }
   CUDA_TRY(cudaGetDevice(&h->device));
   CUDA_TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
-  CUDA_TRY(cudaStreamCreateWithFlags(&h->far2, cudaStreamNonBlocking));
   CUDA_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
-  CUDA_TRY(cudaEventCreateWithFlags(&h->ev_far2, cudaEventDisableTiming));
   try {
     auto store = get_store();
     h->plan = glst::make_plan(natom, tol, box, rcut, ct_float, *store);
@@ -541,7 +603,7 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
   GLST_TRY(dalloc_n(h, &h->sr, (size_t)dev::kSrPlanes * N));
   for (double **o : {&h->cfx, &h->cfy, &h->cfz, &h->cen, &h->ofx, &h->ofy, &h->ofz, &h->oen})
     GLST_TRY(dalloc_n(h, o, N));
-  h->combine_blocks = (uint32_t)std::max<size_t>(1, (N + dev::kCombineThreads - 1) / dev::kCombineThreads);
+  h->combine_blocks = (uint32_t)std::max<size_t>(1, (N + dev::kCombineAtoms - 1) / dev::kCombineAtoms);
   GLST_TRY(dalloc_n(h, &h->block_energy, h->combine_blocks));
   GLST_TRY(dalloc_n(h, &h->energy, 1));
   GLST_TRY(dalloc_n(h, &h->in_host, 4 * N));
@@ -549,7 +611,8 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
   if (K) {
     // Shared-memory plan of the shell-sum kernel: per node a row of ncell+1
     // complex doubles plus its twiddle tables; a few nodes per CTA when the
-    // grid is small (occupancy), one when it is large.
+    // grid is small (occupancy), one when it is large.  Grids whose row does
+    // not fit take the global-memory form (k_gsat_*).
     int smem_optin = 0, nsm = 148;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
     CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
@@ -565,10 +628,9 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
     const size_t xyz_bytes = (C * 4 + 15) & ~size_t(15);
     h->sat_xyz = per_node + xyz_bytes <= smem_total;
     const size_t budget = h->sat_xyz ? smem_total - xyz_bytes : smem_total;
-    if (p.n[0] >= 1024 || p.n[1] >= 1024 || p.n[2] >= 1024 || per_node > budget)
-      return fail(GLST_ERR_SIZE,
-                  "cell grid of %zu cells exceeds the shell-sum shared-memory limit (%zu cells)",
-                  C, budget / sizeof(double2) - 1);
+    const char *force_global = std::getenv("GLST_GLOBAL_SHELL_SUMS");
+    h->gsat = p.n[0] >= 1024 || p.n[1] >= 1024 || p.n[2] >= 1024 || per_node > budget ||
+              (force_global && force_global[0] == '1');
     h->sat_per_node = per_node;
     h->sat_budget = budget;
     h->sat_nb = pow2_floor((uint32_t)std::max<size_t>(1, std::min<size_t>(8, budget / per_node)));
@@ -579,14 +641,22 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
     h->g_kappa_base = kappa_base;
     {
       const Tuning t = tuned(p, h->K);
-      if (t.sat_nb)
+      if (t.sat_nb && !h->gsat)
         h->sat_nb = pow2_floor(std::min<uint32_t>(t.sat_nb, (uint32_t)std::max<size_t>(1, budget / per_node)));
       if (t.lr_waves) h->lr_waves = t.lr_waves;
     }
     GLST_TRY(build_chunks(h, /*in_arena=*/true));
-    const size_t kpad = ((size_t)h->K + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock;
+    const size_t kpad = ((size_t)h->stage_kmax + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock;
     GLST_TRY(dalloc_n(h, &h->S, C * kpad));
     GLST_TRY(dalloc_n(h, &h->R, C * kpad));
+    if (h->gsat) {
+      // tables of a batch of node blocks: ~64 MB (L2-sized) or one block
+      const size_t blk_bytes = C * dev::kNodeBlock * sizeof(double2);
+      const size_t nblk_stage = kpad / dev::kNodeBlock;
+      h->gsat_nblk = (uint32_t)std::max<size_t>(1, std::min<size_t>(nblk_stage, (64ull << 20) / blk_bytes));
+      GLST_TRY(dalloc_n(h, &h->gsat_T, (size_t)h->gsat_nblk * C * dev::kNodeBlock));
+      GLST_TRY(dalloc_n(h, &h->gsat_tw, kpad * (p.n[0] + p.n[1] + p.n[2])));
+    }
   }
   GLST_TRY(commit_allocs(h));
   if (!h->host_chunks.empty()) {
@@ -608,6 +678,7 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
   CUDA_TRY(cudaMemsetAsync(h->flags, 0, 4 * sizeof(uint32_t), h->side));
   CUDA_TRY(cudaStreamSynchronize(h->side));  // memory and tables ready for any stream
   h->computed = false;
+  h->assigned = false;
   return GLST_OK;
 }
 
@@ -625,42 +696,68 @@ static glst_status phase_assign(glst_handle *h, const double *rx, const double *
     dev::k_bin<<<nb, 256, 0, st>>>(rx, ry, rz, N, h->grid, h->atom_cell, h->atom_slot, h->cell_count);
     CUDA_TRY(cudaGetLastError());
   }
-  dev::k_scan<<<1, 1024, 0, st>>>(h->cell_count, C, h->cell_point, h->flags);
+  dev::k_scan<<<1, 1024, 0, st>>>(h->cell_count, C, h->cell_point);
   CUDA_TRY(cudaGetLastError());
   if (N) {
     const uint32_t nb = (N + 255) / 256;
     dev::k_scatter<<<nb, 256, 0, st>>>(h->atom_cell, h->atom_slot, h->cell_point, N, h->perm);
     CUDA_TRY(cudaGetLastError());
     dev::k_sort_pack<<<C, 256, dev::kSortCap * sizeof(uint32_t), st>>>(
-        h->perm, h->cell_count, h->cell_point, h->grid, rx, ry, rz, qc, h->sorted_idx, h->pk, h->pd);
+        h->perm, h->cell_count, h->cell_point, h->grid, h->atom_cell, N, rx, ry, rz, qc, h->sorted_idx, h->pk,
+        h->pd);
+    CUDA_TRY(cudaGetLastError());
+  }
+  h->assigned = true;
+  return GLST_OK;
+}
+
+// Far-field phases of one node stage: structure-factor units [u0, u1),
+// shell sums over nodes [kb, ke), long-range chunks [c0, c1).  S and R hold
+// the stage's nodes (local index = node - rg.kb).
+static glst_status sf_stage(glst_handle *h, const glst_handle::FarRange &rg, cudaStream_t st) {
+  if (rg.u1 <= rg.u0 || !h->plan.natom) return GLST_OK;
+  const uint32_t cg = (h->plan.ncell + dev::kSfCellsPerCta - 1) / dev::kSfCellsPerCta;
+  for (uint32_t r0 = 0; r0 < cg; r0 += 65535u) {  // gridDim.y is at most 65,535
+    dim3 grid(rg.u1 - rg.u0, std::min<uint32_t>(cg - r0, 65535u));
+    dev::k_structure_factors<<<grid, dev::kSfThreads, 0, st>>>(h->pk, h->cell_count, h->cell_point, h->grid,
+                                                                h->sf_units + rg.u0, h->dirs, h->kappa, rg.kb,
+                                                                r0 * dev::kSfCellsPerCta, h->S, h->R);
     CUDA_TRY(cudaGetLastError());
   }
   return GLST_OK;
 }
 
-// Far-field phases over a range of the handle's nodes (local, internal
-// order): structure-factor units [u0, u1), shell sums over nodes [kb, ke),
-// long-range chunks [c0, c1).
-static glst_status sf_range(glst_handle *h, uint32_t u0, uint32_t u1, cudaStream_t st) {
-  if (u1 <= u0 || !h->plan.natom) return GLST_OK;
-  const uint32_t cg = (h->plan.ncell + dev::kSfCellsPerCta - 1) / dev::kSfCellsPerCta;
-  if (cg > 65535) return fail(GLST_ERR_SIZE, "too many cells for the structure-factor grid");
-  dim3 grid(u1 - u0, cg);
-  dev::k_structure_factors<<<grid, dev::kSfThreads, 0, st>>>(h->pk, h->cell_count, h->cell_point, h->grid,
-                                                              h->sf_units + u0, h->dirs, h->kappa, h->S);
-  CUDA_TRY(cudaGetLastError());
-  return GLST_OK;
-}
-
-static glst_status shell_range(glst_handle *h, uint32_t kb, uint32_t ke, cudaStream_t st) {
+static glst_status shell_stage(glst_handle *h, const glst_handle::FarRange &rg, cudaStream_t st) {
+  const uint32_t kb = rg.kb, ke = rg.ke;
   if (ke <= kb || !h->plan.natom) return GLST_OK;
+  const double4 *n64 = h->node64 + h->k_begin + kb;
+  const uint32_t *radii = h->node_radii + h->k_begin + kb;
+  if (h->gsat) {
+    const uint32_t K = ke - kb, C = h->plan.ncell;
+    const uint32_t naxis = h->grid.nx + h->grid.ny + h->grid.nz;
+    const uint64_t ntw = (uint64_t)K * naxis;
+    dev::k_gsat_twiddles<<<(uint32_t)((ntw + 255) / 256), 256, 0, st>>>(h->grid, n64, K, h->gsat_tw);
+    CUDA_TRY(cudaGetLastError());
+    const uint32_t nblk_all = (K + dev::kNodeBlock - 1) / dev::kNodeBlock;
+    for (uint32_t b0 = 0; b0 < nblk_all; b0 += h->gsat_nblk) {
+      dev::GsatArgs a{h->S, n64, radii, h->gsat_tw, h->gsat_T, h->R, K, b0,
+                      std::min(h->gsat_nblk, nblk_all - b0)};
+      const uint64_t per_line = (uint64_t)a.nblk * dev::kNodeBlock;
+      auto blocks = [](uint64_t threads) { return (uint32_t)((threads + 255) / 256); };
+      dev::k_gsat_z<<<blocks((uint64_t)h->grid.nx * h->grid.ny * per_line), 256, 0, st>>>(h->grid, a);
+      dev::k_gsat_prefix<<<blocks((uint64_t)h->grid.nx * h->grid.nz * per_line), 256, 0, st>>>(h->grid, a, 1);
+      dev::k_gsat_prefix<<<blocks((uint64_t)h->grid.ny * h->grid.nz * per_line), 256, 0, st>>>(h->grid, a, 0);
+      dev::k_gsat_shell<<<blocks((uint64_t)C * per_line), 256, 0, st>>>(h->grid, a);
+      CUDA_TRY(cudaGetLastError());
+    }
+    return GLST_OK;
+  }
   uint32_t lg = 0;
   while ((1u << lg) < h->sat_nb) lg++;
   // the cell-coordinate table serves the several-nodes form only (the
   // one-node form steps its cells' coordinates)
   const bool table = h->sat_xyz && h->sat_nb > 1;
-  dev::SatArgs a{h->S, h->node64 + h->k_begin + kb, h->node_radii + h->k_begin + kb, ke - kb, kb,
-                 h->sat_nb, lg, table ? 1u : 0u, h->sat_stride, h->R};
+  dev::SatArgs a{h->S, n64, radii, ke - kb, 0, h->sat_nb, lg, table ? 1u : 0u, h->sat_stride, h->R};
   const uint32_t nblk = (ke - kb + h->sat_nb - 1) / h->sat_nb;
   const size_t smem = h->sat_per_node * h->sat_nb + (table ? (((size_t)h->plan.ncell * 4 + 15) & ~size_t(15)) : 0);
   // several nodes per CTA: 512 threads, 3 CTAs per SM; one node per CTA
@@ -673,26 +770,56 @@ static glst_status shell_range(glst_handle *h, uint32_t kb, uint32_t ke, cudaStr
   return GLST_OK;
 }
 
-static glst_status lr_range(glst_handle *h, uint32_t c0, uint32_t c1, cudaStream_t st) {
-  if (c1 <= c0 || !h->plan.natom) return GLST_OK;
-  dim3 grid((h->plan.natom + dev::kLrThreads - 1) / dev::kLrThreads, c1 - c0);
+static glst_status lr_stage(glst_handle *h, size_t stage, cudaStream_t st) {
+  const auto &rg = h->ranges[stage];
+  if (rg.c1 <= rg.c0 || !h->plan.natom) return GLST_OK;
+  dim3 grid((h->plan.natom + dev::kLrThreads - 1) / dev::kLrThreads, rg.c1 - rg.c0);
+  // stage 0 writes its rows, later stages add into the same rows
   dev::k_long_range_flat<<<grid, dev::kLrThreads, 0, st>>>(
-      h->pk, h->cell_point, h->plan.ncell, h->chunks + c0, h->dirs, h->kappa, h->R, h->plan.natom,
-      h->part + (size_t)c0 * h->plan.natom);
+      h->pk, h->cell_point, h->plan.ncell, h->chunks + rg.c0, h->dirs, h->kappa, h->R, rg.kb, h->plan.natom,
+      stage > 0 ? 1 : 0, h->part);
   CUDA_TRY(cudaGetLastError());
   return GLST_OK;
 }
 
+// Rows that a later stage accumulates into but stage 0 does not write.
+static glst_status zero_part_tail(glst_handle *h, cudaStream_t st) {
+  if (h->part_zero_from < h->part_rows && h->plan.natom)
+    CUDA_TRY(cudaMemsetAsync(h->part + (size_t)h->part_zero_from * h->plan.natom, 0,
+                             (size_t)(h->part_rows - h->part_zero_from) * h->plan.natom * sizeof(double4), st));
+  return GLST_OK;
+}
+
+// The far field of every stage, in order, on one stream.
+static glst_status far_all(glst_handle *h, cudaStream_t st) {
+  if (!h->K || !h->plan.natom) return GLST_OK;
+  GLST_TRY(zero_part_tail(h, st));
+  for (size_t r = 0; r < h->ranges.size(); r++) {
+    GLST_TRY(sf_stage(h, h->ranges[r], st));
+    GLST_TRY(shell_stage(h, h->ranges[r], st));
+    GLST_TRY(lr_stage(h, r, st));
+  }
+  return GLST_OK;
+}
+
+// The reference's phase methods.  With one node stage each runs its own
+// kernel; with several (S and R hold one stage at a time) calc_sf runs the
+// whole far field stage by stage and sum_rmt_sf / calc_lr_ef have nothing
+// left to do -- the results are the same as the fused call's.
+static bool single_stage(const glst_handle *h) { return h->ranges.size() <= 1; }
+
 static glst_status phase_sf(glst_handle *h, cudaStream_t st) {
-  return h->K ? sf_range(h, 0, h->n_sf_units, st) : GLST_OK;
+  if (!h->K) return GLST_OK;
+  if (!single_stage(h)) return far_all(h, st);
+  return sf_stage(h, h->ranges[0], st);
 }
 
 static glst_status phase_shell(glst_handle *h, cudaStream_t st) {
-  return h->K ? shell_range(h, 0, h->K, st) : GLST_OK;
+  return (h->K && single_stage(h)) ? shell_stage(h, h->ranges[0], st) : GLST_OK;
 }
 
 static glst_status phase_lr(glst_handle *h, cudaStream_t st) {
-  return h->K ? lr_range(h, 0, h->nsplit, st) : GLST_OK;
+  return (h->K && single_stage(h)) ? lr_stage(h, 0, st) : GLST_OK;
 }
 
 static glst_status phase_sr(glst_handle *h, cudaStream_t st) {
@@ -708,7 +835,7 @@ static glst_status phase_combine(glst_handle *h, cudaStream_t st) {
   const uint32_t N = h->plan.natom;
   if (N) {
     dev::k_combine<<<h->combine_blocks, dev::kCombineThreads, 0, st>>>(
-        h->sr, h->part, h->nsplit, h->sorted_idx, N, h->K ? 1 : 0, h->cfx, h->cfy, h->cfz, h->cen,
+        h->sr, h->part, h->part_rows, h->sorted_idx, N, h->K ? 1 : 0, h->cfx, h->cfy, h->cfz, h->cen,
         h->ofx, h->ofy, h->ofz, h->oen, h->block_energy);
     CUDA_TRY(cudaGetLastError());
     dev::k_energy_total<<<1, 256, 0, st>>>(h->block_energy, h->combine_blocks, h->energy);
@@ -723,44 +850,34 @@ static glst_status phase_combine(glst_handle *h, cudaStream_t st) {
 static glst_status compute_all(glst_handle *h, const double *rx, const double *ry, const double *rz,
                                const double *qc, cudaStream_t st) {
   GLST_TRY(phase_assign(h, rx, ry, rz, qc, st));
-  CUDA_TRY(cudaEventRecord(h->ev_fork, st));
   // The near field (FP64 pipe) runs on a side stream, overlapping the far
-  // field on the same SMs.  It is forked after the structure factors, so it
-  // shares the SMs with the shell sums and the gather: measured on water10k
-  // 3.336 ms per solve against 3.375 ms forked before the structure factors
-  // (whose FMA and SFU pipes it slowed) and 3.52 ms after the shell sums.
+  // field on the same SMs.  It is forked after the (first stage's) structure
+  // factors, so it shares the SMs with the shell sums and the gather:
+  // measured on water10k 3.336 ms per solve against 3.375 ms forked before
+  // the structure factors (whose FMA and SFU pipes it slowed) and 3.52 ms
+  // after the shell sums.  (Splitting one system's far field over two
+  // streams measured no overlap: the structure-factor kernel fills every
+  // SM's register file, so the other stream's blocks only start as it
+  // drains; water10k 3.27-3.42 ms per solve at 2-8 node ranges against 3.14.)
   bool sr_forked = false;
-  auto fork_sr = [&](cudaStream_t s) -> glst_status {
-    CUDA_TRY(cudaEventRecord(h->ev_fork, s));
+  auto fork_sr = [&]() -> glst_status {
+    CUDA_TRY(cudaEventRecord(h->ev_fork, st));
     CUDA_TRY(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
     GLST_TRY(phase_sr(h, h->side));
     CUDA_TRY(cudaEventRecord(h->ev_join, h->side));
     sr_forked = true;
     return GLST_OK;
   };
-  // Far field in node ranges, alternating between two streams so that the
-  // shell sums of one range (shared-memory bound) could overlap the SFU-bound
-  // kernels of the next.  Measured on B200 it does not: the structure-factor
-  // kernel fills every SM's register file, so the other stream's blocks only
-  // start as it drains.  Nor does putting every stage's structure factors on
-  // this stream and each stage's shell sums and gather behind them on a
-  // highest-priority stream (water10k 3.27 / 3.35 / 3.42 ms per solve at 2 /
-  // 4 / 8 stages against 3.14 ms).  kFarStages is therefore 1 (the plain
-  // sequence).
   if (h->K && h->plan.natom && !h->ranges.empty()) {
-    CUDA_TRY(cudaStreamWaitEvent(h->far2, h->ev_fork, 0));
+    GLST_TRY(zero_part_tail(h, st));
     for (size_t r = 0; r < h->ranges.size(); r++) {
-      const auto &rg = h->ranges[r];
-      cudaStream_t s = (r & 1) ? h->far2 : st;
-      GLST_TRY(sf_range(h, rg.u0, rg.u1, s));
-      if (!sr_forked) GLST_TRY(fork_sr(s));
-      GLST_TRY(shell_range(h, rg.kb, rg.ke, s));
-      GLST_TRY(lr_range(h, rg.c0, rg.c1, s));
+      GLST_TRY(sf_stage(h, h->ranges[r], st));
+      if (!sr_forked) GLST_TRY(fork_sr());
+      GLST_TRY(shell_stage(h, h->ranges[r], st));
+      GLST_TRY(lr_stage(h, r, st));
     }
-    CUDA_TRY(cudaEventRecord(h->ev_far2, h->far2));
-    CUDA_TRY(cudaStreamWaitEvent(st, h->ev_far2, 0));
   }
-  if (!sr_forked) GLST_TRY(fork_sr(st));
+  if (!sr_forked) GLST_TRY(fork_sr());
   CUDA_TRY(cudaStreamWaitEvent(st, h->ev_join, 0));
   return phase_combine(h, st);
 }
@@ -1000,9 +1117,18 @@ glst_status glst_get_info(const glst_handle *h, glst_info *info) {
   DeviceGuard guard_(h);
   fill_info(h->plan, info);
   info->device_bytes = h->bytes;
-  // assignment 4 (+0 without atoms), near field 1, far field 3 per stage, combine 2
-  info->kernels_per_compute =
-      h->plan.natom ? 4u + (h->shard == 0 ? 1u : 0u) + 3u * (uint32_t)(h->K ? h->ranges.size() : 0) + 2u : 2u;
+  // assignment 4 (+0 without atoms), near field 1, far field per stage:
+  // structure factors 1, shell sums 1 (global-memory form: twiddles 1 + 4
+  // per node batch), gather 1; combine 2
+  uint32_t far = 0;
+  if (h->K && h->plan.natom)
+    for (const auto &rg : h->ranges) {
+      const uint32_t nblk = (rg.ke - rg.kb + dev::kNodeBlock - 1) / dev::kNodeBlock;
+      far += 2u + (h->gsat ? 1u + 4u * ((nblk + h->gsat_nblk - 1) / h->gsat_nblk) : 1u);
+    }
+  info->kernels_per_compute = h->plan.natom ? 4u + (h->shard == 0 ? 1u : 0u) + far + 2u : 2u;
+  info->node_stages = (uint32_t)h->ranges.size();
+  info->shell_sums_global = h->gsat ? 1u : 0u;
   return GLST_OK;
 }
 
@@ -1050,7 +1176,7 @@ glst_status glst_autotune(glst_handle *h, const double *rx, const double *ry, co
   if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
   DeviceGuard guard_(h);
   cudaStream_t st = S_(stream);
-  if (h->K && h->plan.natom && h->nshards == 1) {
+  if (h->K && h->plan.natom && h->nshards == 1 && single_stage(h)) {
     GLST_TRY(phase_assign(h, rx, ry, rz, qc, st));
     GLST_TRY(phase_sf(h, st));
     cudaEvent_t a, b;
@@ -1069,7 +1195,7 @@ glst_status glst_autotune(glst_handle *h, const double *rx, const double *ry, co
     uint32_t best_nb = h->sat_nb;
     float best = 1e30f;
     for (uint32_t nb : {1u, 2u, 4u, 8u, 16u, 32u}) {
-      if (h->sat_per_node * nb > h->sat_budget) break;
+      if (h->gsat || h->sat_per_node * nb > h->sat_budget) break;
       h->sat_nb = nb;
       float ms = 0.f;
       GLST_TRY(timed(phase_shell, &ms));
@@ -1152,10 +1278,67 @@ glst_status glst_check(glst_handle *h, void *stream) {
   uint32_t flags[4] = {0, 0, 0, 0};
   CUDA_TRY(cudaMemcpyAsync(flags, h->flags, sizeof flags, cudaMemcpyDeviceToHost, S_(stream)));
   CUDA_TRY(cudaStreamSynchronize(S_(stream)));
-  if (flags[0] & dev::kFlagCellOverflow)
-    return fail(GLST_ERR_SIZE,
-                "a cell holds more than %u atoms: energies and forces are valid but the "
-                "order of atoms inside that cell is not the reference's", dev::kSortCap);
+  if (flags[0]) return fail(GLST_ERR_STATE, "device error flags 0x%x raised by the last compute", flags[0]);
+  return GLST_OK;
+}
+
+glst_status glst_get_far_field(glst_handle *h, double *sf_re, double *sf_im, double *rmt_re, double *rmt_im,
+                               void *stream) {
+  if (!h) return fail(GLST_ERR_INVALID_ARG, "null handle");
+  DeviceGuard guard_(h);
+  if (h->nshards > 1) return fail(GLST_ERR_STATE, "far-field arrays are available for whole-system handles only");
+  if (!h->assigned) return fail(GLST_ERR_STATE, "far-field arrays requested before positions were assigned");
+  const Plan &p = h->plan;
+  const size_t C = p.ncell, K = p.has_far ? p.K() : 0;
+  double *outs[4] = {sf_re, sf_im, rmt_re, rmt_im};
+  for (double *o : outs)
+    if (o) std::fill(o, o + C * K, 0.0);
+  if (!K || !p.natom) return GLST_OK;
+  cudaStream_t st = S_(stream);
+  // internal node (group -> direction -> radial) -> reference index (group ->
+  // radial -> direction, src/cubature.cu:120-145), and the node vector as the
+  // device holds it (rounded to CT)
+  std::vector<uint32_t> ref_of(K);
+  {
+    size_t base = 0;
+    for (const auto &g : p.groups) {
+      for (uint32_t j = 0; j < g.n_dir; j++)
+        for (uint32_t r = 0; r < g.n_radial; r++)
+          ref_of[base + (size_t)j * g.n_radial + r] = (uint32_t)(base + (size_t)r * g.n_dir + j);
+      base += (size_t)g.n_radial * g.n_dir;
+    }
+  }
+  auto ct = [&](double v) { return p.ct_float ? (double)(float)v : v; };
+  const double l = h->grid.l;
+  std::vector<float2> hs, hr;
+  for (const auto &rg : h->ranges) {
+    const size_t nk = rg.ke - rg.kb;
+    const size_t nel = C * ((nk + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock);
+    GLST_TRY(sf_stage(h, rg, st));
+    GLST_TRY(shell_stage(h, rg, st));
+    hs.resize(nel);
+    hr.resize(nel);
+    CUDA_TRY(cudaMemcpyAsync(hs.data(), h->S, nel * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(hr.data(), h->R, nel * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    for (size_t kl = 0; kl < nk; kl++) {
+      const size_t ref = ref_of[rg.kb + kl];
+      const double kx = ct(p.kx[ref]), ky = ct(p.ky[ref]), kz = ct(p.kz[ref]);
+      for (size_t c = 0; c < C; c++) {
+        const uint32_t x = (uint32_t)(c / ((size_t)p.n[1] * p.n[2])), y = (uint32_t)((c / p.n[2]) % p.n[1]),
+                       z = (uint32_t)(c % p.n[2]);
+        const double ph = kx * ((x + 0.5) * l) + ky * ((y + 0.5) * l) + kz * ((z + 0.5) * l);
+        const double cs = std::cos(ph), sn = -std::sin(ph);  // e^{-ik.c}
+        const float2 a = hs[dev::sr_index((uint32_t)c, (uint32_t)kl, (uint32_t)C)];
+        const float2 b = hr[dev::sr_index((uint32_t)c, (uint32_t)kl, (uint32_t)C)];
+        const size_t o = c * K + ref;
+        if (sf_re) sf_re[o] = a.x * cs - a.y * sn;
+        if (sf_im) sf_im[o] = a.x * sn + a.y * cs;
+        if (rmt_re) rmt_re[o] = b.x * cs - b.y * sn;
+        if (rmt_im) rmt_im[o] = b.x * sn + b.y * cs;
+      }
+    }
+  }
   return GLST_OK;
 }
 
@@ -1444,8 +1627,16 @@ uint64_t estimate_bytes(const Plan &p, int nsm) {
   if (K) {
     const uint64_t slots = (uint64_t)nsm * 16;
     const uint64_t chunks = std::max<uint64_t>(1, (8 * slots + C - 1) / C) + p.groups.size() + 1;
-    b += K * (32 + 4 + 16 + 4) + C * ((K + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock) * (8 + 8) +
-         chunks * N * 32;
+    const uint64_t kpad = (K + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock;
+    const uint64_t nst = std::max<uint64_t>(1, (C * kpad * 16 + stage_budget() - 1) / stage_budget());
+    // the largest stage: ~K / stages, plus up to one direction's nodes
+    const uint64_t stage_k = std::min<uint64_t>(kpad, (K + nst - 1) / nst + 2 * dev::kLrfTileNodes);
+    const uint64_t stage_kpad = (stage_k + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock;
+    b += K * (32 + 4 + 16 + 4) + C * stage_kpad * (8 + 8) + chunks * N * 32;
+    // global-memory shell-sum tables (grids whose per-node table exceeds the
+    // shared memory of a CTA): 64 MB or one block, and the twiddles
+    if ((C + 9 + p.n[0] + p.n[1] + p.n[2]) * 16 > (200ull << 10))
+      b += std::max<uint64_t>(64ull << 20, C * dev::kNodeBlock * 16) + stage_kpad * (p.n[0] + p.n[1] + p.n[2]) * 16;
   }
   return b + 64 * 16 * 64;  // per-buffer allocation granularity
 }

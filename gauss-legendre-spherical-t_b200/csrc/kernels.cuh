@@ -4,9 +4,11 @@
 //   pk[N]      float4 (dx, dy, dz, q): cell-ordered atoms, position relative
 //              to the centre of the atom's cell, computed in FP64 and rounded
 //   pd[N]      double4 (x, y, z, q): cell-ordered atoms, FP64 absolute
-//   S[C][K]    double2: structure factor of every cell at every node
+//   S[C][K]    float2: cell-relative structure factor sum_j q_j e^{-ik.(r_j - c)}
+//              of every cell at every node (FP32 per atom tile, FP64 across
+//              tiles, stored rounded to FP32)
 //   R[C][K]    float2: shell sum times weight times e^{+ik.c} (cell centre c)
-//   part[P][N] double4: long-range partial sums, one row per node split
+//   part[P][N] double4: long-range partial sums, one row per node chunk
 //   sr[N]      double4: near-field sums
 // Cell c = (ix*ny + iy)*nz + iz, as in the reference (src/glst_force.cu:379-382).
 #pragma once
@@ -17,8 +19,7 @@
 namespace glst {
 namespace dev {
 
-constexpr unsigned kSortCap = 8192;   // atoms per cell the cell sort can hold
-constexpr unsigned kFlagCellOverflow = 1u;
+constexpr unsigned kSortCap = 8192;   // atoms per cell the shared-memory cell sort holds
 
 struct Grid {
   uint32_t nx, ny, nz, ncell;
@@ -84,19 +85,17 @@ __global__ void k_bin(const double *__restrict__ rx, const double *__restrict__ 
 }
 
 // K_scan: exclusive offsets of the cell counts (one CTA of 1024 threads,
-// chunked block scan), and the error flag for cells the sort cannot hold.
+// chunked block scan).
 __global__ void k_scan(const uint32_t *__restrict__ cell_count, uint32_t ncell,
-                       uint32_t *__restrict__ cell_point, uint32_t *__restrict__ flags) {
+                       uint32_t *__restrict__ cell_point) {
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t carry;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  bool overflow = false;
   for (uint32_t base = 0; base < ncell; base += blockDim.x) {
     const uint32_t c = base + threadIdx.x;
     const uint32_t v = (c < ncell) ? cell_count[c] : 0u;
-    overflow |= (v > kSortCap);
     uint32_t x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -122,7 +121,6 @@ __global__ void k_scan(const uint32_t *__restrict__ cell_count, uint32_t ncell,
     if (threadIdx.x == blockDim.x - 1) carry = before + v;
     __syncthreads();
   }
-  if (__syncthreads_or(overflow) && threadIdx.x == 0) atomicOr(flags, kFlagCellOverflow);
 }
 
 __global__ void k_scatter(const uint32_t *__restrict__ atom_cell,
@@ -137,10 +135,24 @@ __global__ void k_scatter(const uint32_t *__restrict__ atom_cell,
 // K_sort_pack: one CTA per cell.  The atomics of k_bin leave the atoms of a
 // cell in arbitrary order; sorting each cell's indices ascending reproduces
 // the order of a stable sort by cell id (the reference's CUB radix sort,
-// src/glst_force.cu:510-517).  Then writes the packets.
+// src/glst_force.cu:510-517).  Then writes the packets.  Launched with
+// blockDim.x a multiple of 32 and kSortCap u32 of dynamic shared memory.
+__device__ __forceinline__ void pack_atom(uint32_t slot, uint32_t a, double cx, double cy, double cz,
+                                          const double *__restrict__ rx, const double *__restrict__ ry,
+                                          const double *__restrict__ rz, const double *__restrict__ qc,
+                                          uint32_t *__restrict__ sorted_idx, float4 *__restrict__ pk,
+                                          double4 *__restrict__ pd) {
+  const double x = rx[a], y = ry[a], z = rz[a], q = qc[a];
+  sorted_idx[slot] = a;
+  pd[slot] = make_double4(x, y, z, q);
+  pk[slot] = make_float4(static_cast<float>(x - cx), static_cast<float>(y - cy), static_cast<float>(z - cz),
+                         static_cast<float>(q));
+}
+
 __global__ void k_sort_pack(const uint32_t *__restrict__ perm,
                             const uint32_t *__restrict__ cell_count,
                             const uint32_t *__restrict__ cell_point, Grid g,
+                            const uint32_t *__restrict__ atom_cell, uint32_t natom,
                             const double *__restrict__ rx, const double *__restrict__ ry,
                             const double *__restrict__ rz, const double *__restrict__ qc,
                             uint32_t *__restrict__ sorted_idx, float4 *__restrict__ pk,
@@ -153,16 +165,31 @@ __global__ void k_sort_pack(const uint32_t *__restrict__ perm,
   const uint32_t ix = cell / (g.ny * g.nz), iy = (cell / g.nz) % g.ny, iz = cell % g.nz;
   const double cx = cell_centre(ix, g.l), cy = cell_centre(iy, g.l), cz = cell_centre(iz, g.l);
   if (cnt > kSortCap) {
-    // Too many atoms to sort in shared memory: pack in slot order (physics
-    // unchanged, within-cell order not the reference's; k_scan flagged it).
-    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
-      const uint32_t a = perm[start + i];
-      const double x = rx[a], y = ry[a], z = rz[a], q = qc[a];
-      sorted_idx[start + i] = a;
-      pd[start + i] = make_double4(x, y, z, q);
-      pk[start + i] = make_float4(static_cast<float>(x - cx), static_cast<float>(y - cy),
-                                  static_cast<float>(z - cz), static_cast<float>(q));
+    // Too many atoms for the shared-memory sort: an atom's place in the cell
+    // is the number of atoms of the cell with a smaller index, found by one
+    // pass over every atom's cell in index order (per step: a warp ballot per
+    // warp, then the counts of the warps before).  Stable by construction;
+    // O(natom) per such cell, which only dense grids have.
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t seen = 0;
+    for (uint32_t i0 = 0; i0 < natom; i0 += blockDim.x) {
+      const uint32_t i = i0 + threadIdx.x;
+      const bool mine = i < natom && atom_cell[i] == cell;
+      const uint32_t bal = __ballot_sync(0xffffffffu, mine);
+      if (lane == 0) s_idx[warp] = __popc(bal);
+      __syncthreads();
+      uint32_t before = seen, total = seen;
+      for (uint32_t w = 0; w < nw; w++) {
+        const uint32_t c = s_idx[w];
+        before += (w < warp) ? c : 0u;
+        total += c;
+      }
+      if (mine) sorted_idx[start + before + __popc(bal & ((1u << lane) - 1u))] = i;
+      seen = total;
+      __syncthreads();
     }
+    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
+      pack_atom(start + i, sorted_idx[start + i], cx, cy, cz, rx, ry, rz, qc, sorted_idx, pk, pd);
     return;
   }
   uint32_t np2 = 1;
@@ -187,14 +214,8 @@ __global__ void k_sort_pack(const uint32_t *__restrict__ perm,
       __syncthreads();
     }
   }
-  for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
-    const uint32_t a = s_idx[i];
-    const double x = rx[a], y = ry[a], z = rz[a], q = qc[a];
-    sorted_idx[start + i] = a;
-    pd[start + i] = make_double4(x, y, z, q);
-    pk[start + i] = make_float4(static_cast<float>(x - cx), static_cast<float>(y - cy),
-                                static_cast<float>(z - cz), static_cast<float>(q));
-  }
+  for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
+    pack_atom(start + i, s_idx[i], cx, cy, cz, rx, ry, rz, qc, sorted_idx, pk, pd);
 }
 
 // ----------------------------------------------------------------------------
@@ -269,9 +290,9 @@ __device__ __forceinline__ void fma_sincos_signed2(float2 th, float q, float2 *s
 // kSfCellsPerCta consecutive cells.  Per (atom, node): one multiply, a sine
 // and cosine (SFU, or the FMA-pipe polynomial for the last slot pairs), two
 // FMAs, in paired FP32 instructions where two slots go together.  FP32 over a
-// tile of <= kSfAtomTile atoms (|k.d| <~ 25 rad), then FP64 over tiles.  S
-// is stored cell-relative; its twiddle e^{-ik.c} is applied by the shell-sum
-// kernel as it loads S.
+// tile of <= kSfAtomTile atoms (|k.d| <~ 25 rad), then FP64 over the tiles of
+// a denser cell.  S is stored cell-relative in FP32; its twiddle e^{-ik.c}
+// is applied by the shell-sum kernel as it loads S.
 constexpr int kSfThreads = 128;
 constexpr int kSfMaxNpt = 12;     // radial nodes per thread, at most
 constexpr int kSfCellsPerCta = 2;
@@ -299,13 +320,37 @@ struct SfUnit {
 // (npt - 1) / 4, 1.30 with (npt + 1) / 4.
 __host__ __device__ constexpr int sf_poly_pairs(int npt) { return (npt - 3) / 4; }
 
+// A cell of several tiles adds them in FP64: the running sum is kept between
+// tiles as an unevaluated pair of floats, the leading part in S and the
+// remainder in lo_buf (the shell sums' output buffer, which is free until
+// the structure factors are done); the last tile stores the sum rounded once
+// to FP32.  Out of line, so that the registers of this rare path do not
+// count against the hot loop's.
+__device__ __noinline__ void sf_store_dense(const float2 *s_f, uint32_t nodes, uint32_t cell, uint32_t node0,
+                                            uint32_t ncell, bool add, bool last, float2 *__restrict__ S,
+                                            float2 *__restrict__ lo_buf) {
+  for (uint32_t m = threadIdx.x; m < nodes; m += kSfThreads) {
+    const size_t o = sr_index(cell, node0 + m, ncell);
+    const float2 f = s_f[m];
+    double vx = f.x, vy = f.y;
+    if (add) {
+      const float2 h = S[o], l = lo_buf[o];
+      vx += (double)h.x + (double)l.x;
+      vy += (double)h.y + (double)l.y;
+    }
+    const float hx = static_cast<float>(vx), hy = static_cast<float>(vy);
+    S[o] = make_float2(hx, hy);
+    if (!last) lo_buf[o] = make_float2(static_cast<float>(vx - hx), static_cast<float>(vy - hy));
+  }
+}
+
 template <int NPT>
 __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restrict__ pk,
                                         const uint32_t *__restrict__ cell_count,
                                         const uint32_t *__restrict__ cell_point, const Grid &g,
                                         const float4 *__restrict__ dirs, const float *__restrict__ kappa,
-                                        uint32_t c0,
-                                        uint32_t c1, float2 *__restrict__ S, float4 *s_at, float2 *s_f) {
+                                        uint32_t c0, uint32_t c1, uint32_t node_off, float2 *__restrict__ S,
+                                        float2 *__restrict__ lo_buf, float4 *s_at, float2 *s_f) {
   // Slots are handled in pairs (FMUL2/FFMA2); an odd last slot alone.
   constexpr int NP2 = NPT / 2;
   constexpr bool ODD = (NPT & 1) != 0;
@@ -372,11 +417,11 @@ __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restric
         }
       }
       // Tile sums to shared memory in the unit's node order, then one thread
-      // per node (coalesced): S store or add.  S holds the cell-relative
-      // sums in FP32 (each is an FP32 tile sum already; FP64 storage held no
-      // more information and doubled the bytes written here and read by the
-      // shell sums); the shell-sum kernel applies the twiddle e^{-ik.c} in
-      // FP64 from its per-axis tables as it loads S.
+      // per node (coalesced) stores them.  S holds the cell-relative sums in
+      // FP32 (an FP32 tile sum; FP64 storage held no more information and
+      // doubled the bytes written here and read by the shell sums); the
+      // shell-sum kernel applies the twiddle e^{-ik.c} in FP64 from its
+      // per-axis tables as it loads S.
       if (act) {
 #pragma unroll
         for (int k = 0; k < NP2; k++) {
@@ -386,35 +431,34 @@ __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restric
         if (ODD && r0 + NPT - 1 < u.n_rad) s_f[d * u.n_rad + r0 + NPT - 1] = make_float2(fr_odd, -fi_odd);
       }
       __syncthreads();
-      for (uint32_t m = threadIdx.x; m < nodes; m += kSfThreads) {
-        const uint32_t k = u.node_begin + m;
-        const float2 f = s_f[m];
-        float2 *dst = S + sr_index(cell, k, g.ncell);
-        if (a0 == 0) {
-          *dst = f;
-        } else {
-          const float2 o = *dst;
-          *dst = make_float2(o.x + f.x, o.y + f.y);
-        }
+      if (cnt <= kSfAtomTile) {
+        for (uint32_t m = threadIdx.x; m < nodes; m += kSfThreads)
+          S[sr_index(cell, u.node_begin + m - node_off, g.ncell)] = s_f[m];
+      } else {
+        sf_store_dense(s_f, nodes, cell, u.node_begin - node_off, g.ncell, a0 > 0, a0 + kSfAtomTile >= cnt, S,
+                       lo_buf);
       }
       a0 += kSfAtomTile;
     } while (a0 < cnt);
   }
 }
 
-// Units index S by local node.
+// Units index nodes by the handle's local node; S holds the nodes from
+// node_off on (a node range of the handle: the whole of it, or one stage).
+// Cells: kSfCellsPerCta per CTA row from cell_base on (grids of more than
+// 65,535 rows take several launches).  lo_buf: scratch of S's size.
 __global__ void __launch_bounds__(kSfThreads, 8)
 k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_count,
                     const uint32_t *__restrict__ cell_point, Grid g, const SfUnit *__restrict__ units,
-                    const float4 *__restrict__ dirs, const float *__restrict__ kappa,
-                    float2 *__restrict__ S) {
+                    const float4 *__restrict__ dirs, const float *__restrict__ kappa, uint32_t node_off,
+                    uint32_t cell_base, float2 *__restrict__ S, float2 *__restrict__ lo_buf) {
   __shared__ float4 s_at[kSfAtomTile];
   __shared__ float2 s_f[kSfThreads * kSfMaxNpt];
   const SfUnit u = units[blockIdx.x];
-  const uint32_t c0 = blockIdx.y * kSfCellsPerCta;
+  const uint32_t c0 = cell_base + blockIdx.y * kSfCellsPerCta;
   const uint32_t c1 = min(g.ncell, c0 + kSfCellsPerCta);
 #define GLST_SF_CASE(n) \
-  case n: sf_unit<n>(u, pk, cell_count, cell_point, g, dirs, kappa, c0, c1, S, s_at, s_f); break;
+  case n: sf_unit<n>(u, pk, cell_count, cell_point, g, dirs, kappa, c0, c1, node_off, S, lo_buf, s_at, s_f); break;
   switch (u.npt) {
     GLST_SF_CASE(1) GLST_SF_CASE(2) GLST_SF_CASE(3) GLST_SF_CASE(4) GLST_SF_CASE(5) GLST_SF_CASE(6)
     GLST_SF_CASE(7) GLST_SF_CASE(8) GLST_SF_CASE(9) GLST_SF_CASE(10) GLST_SF_CASE(11) GLST_SF_CASE(12)
@@ -627,6 +671,154 @@ k_shell_sums(Grid g, SatArgs a) {
 }
 
 // ----------------------------------------------------------------------------
+// Shell sums for grids whose per-node prefix table does not fit in shared
+// memory (the same arithmetic as k_shell_sums, src/glst_force.cu:702-913):
+// the FP64 summed-area tables of a batch of node blocks live in global memory
+// (laid out like S: per block of kNodeBlock nodes, cell-major, node fastest,
+// so every warp access is a contiguous run of 32 nodes), built by three
+// line passes (z with the twiddle e^{-ik.c} applied on load, then y, then x)
+// and read by a fourth pass that forms the 16-corner shell differences.  The
+// per-axis twiddles of the stage's nodes are tabulated once per stage.
+struct GsatArgs {
+  const float2 *S;              // stage-local structure factors
+  const double4 *node64;        // node table of the stage (kx, ky, kz, w)
+  const uint32_t *node_radii;   // r_in | r_out << 16, same indexing
+  const double2 *tw;            // per stage node: nx + ny + nz twiddles e^{+i k_a c_a}
+  double2 *T;                   // tables of the batch: nblk x C x kNodeBlock
+  float2 *R;                    // stage-local shell sums
+  uint32_t K;                   // nodes of the stage
+  uint32_t blk0;                // first node block of the batch (stage-local)
+  uint32_t nblk;                // node blocks in the batch
+};
+
+// Twiddle table: tw[k * (nx + ny + nz) + a] = e^{+i k_axis (i + 1/2) l}.
+__global__ void k_gsat_twiddles(Grid g, const double4 *__restrict__ node64, uint32_t K,
+                                double2 *__restrict__ tw) {
+  const uint32_t naxis = g.nx + g.ny + g.nz;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)K * naxis) return;
+  const uint32_t k = (uint32_t)(t / naxis), r = (uint32_t)(t - (size_t)k * naxis);
+  const double4 nk = node64[k];
+  double kc;
+  if (r < g.nx) kc = nk.x * cell_centre(r, g.l);
+  else if (r < g.nx + g.ny) kc = nk.y * cell_centre(r - g.nx, g.l);
+  else kc = nk.z * cell_centre(r - g.nx - g.ny, g.l);
+  double sn, cs;
+  sincos(kc, &sn, &cs);
+  tw[t] = make_double2(cs, sn);
+}
+
+__device__ __forceinline__ size_t gsat_at(uint32_t bb, uint32_t c, uint32_t j, uint32_t C) {
+  return ((size_t)bb * C + c) * kNodeBlock + j;
+}
+
+// Pass 1: thread = (line (x, y), block, node j); S x e^{-ik.c}, prefix along z.
+__global__ void k_gsat_z(Grid g, GsatArgs a) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t j = (uint32_t)(t % kNodeBlock);
+  const size_t lb = t / kNodeBlock;
+  const uint32_t bb = (uint32_t)(lb % a.nblk);
+  const size_t line = lb / a.nblk;
+  if (line >= (size_t)g.nx * g.ny) return;
+  const uint32_t blk = a.blk0 + bb;
+  const uint32_t k = blk * kNodeBlock + j;  // stage-local node
+  const uint32_t C = g.ncell, naxis = g.nx + g.ny + g.nz;
+  const uint32_t x = (uint32_t)(line / g.ny), y = (uint32_t)(line - (size_t)x * g.ny);
+  const uint32_t c0 = (uint32_t)line * g.nz;
+  double2 *T = a.T;
+  if (k >= a.K) {
+    for (uint32_t z = 0; z < g.nz; z++) T[gsat_at(bb, c0 + z, j, C)] = make_double2(0.0, 0.0);
+    return;
+  }
+  const double2 *tk = a.tw + (size_t)k * naxis;
+  const double2 txy = cmul(tk[x], tk[g.nx + y]);
+  const double2 *twz = tk + g.nx + g.ny;
+  double2 acc = make_double2(0.0, 0.0);
+#pragma unroll 4
+  for (uint32_t z = 0; z < g.nz; z++) {
+    const float2 v = a.S[sr_index(c0 + z, k, C)];
+    const double2 tt = cmul(txy, twz[z]);
+    const double vx = v.x, vy = v.y;
+    acc.x += vx * tt.x + vy * tt.y;  // v * conj(tt)
+    acc.y += vy * tt.x - vx * tt.y;
+    T[gsat_at(bb, c0 + z, j, C)] = acc;
+  }
+}
+
+// Passes 2 and 3: prefix along y (axis 1) or x (axis 0), in place.
+__global__ void k_gsat_prefix(Grid g, GsatArgs a, int axis) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t j = (uint32_t)(t % kNodeBlock);
+  const size_t lb = t / kNodeBlock;
+  const uint32_t bb = (uint32_t)(lb % a.nblk);
+  const size_t line = lb / a.nblk;
+  const uint32_t C = g.ncell;
+  uint32_t n, c0, stride;
+  if (axis == 1) {  // lines (x, z)
+    if (line >= (size_t)g.nx * g.nz) return;
+    const uint32_t x = (uint32_t)(line / g.nz), z = (uint32_t)(line - (size_t)x * g.nz);
+    n = g.ny; c0 = x * g.ny * g.nz + z; stride = g.nz;
+  } else {  // lines (y, z)
+    if (line >= (size_t)g.ny * g.nz) return;
+    n = g.nx; c0 = (uint32_t)line; stride = g.ny * g.nz;
+  }
+  double2 *T = a.T;
+  double2 acc = make_double2(0.0, 0.0);
+#pragma unroll 4
+  for (uint32_t i = 0; i < n; i++) {
+    double2 *p = T + gsat_at(bb, c0 + i * stride, j, C);
+    const double2 v = *p;
+    acc.x += v.x;
+    acc.y += v.y;
+    *p = acc;
+  }
+}
+
+__device__ __forceinline__ double2 gcube_sum(const double2 *T, uint32_t bb, uint32_t j, uint32_t x, uint32_t y,
+                                             uint32_t z, uint32_t r, const Grid &g) {
+  const uint32_t C = g.ncell;
+  const uint32_t x0 = (x < r) ? 0 : x - r, y0 = (y < r) ? 0 : y - r, z0 = (z < r) ? 0 : z - r;
+  const uint32_t x1 = min(x + r, g.nx - 1), y1 = min(y + r, g.ny - 1), z1 = min(z + r, g.nz - 1);
+  const bool xb = x0 == 0, yb = y0 == 0, zb = z0 == 0;
+  const uint32_t xm = xb ? 0 : x0 - 1, ym = yb ? 0 : y0 - 1, zm = zb ? 0 : z0 - 1;
+  auto at = [&](uint32_t a, uint32_t b, uint32_t c) { return T[gsat_at(bb, (a * g.ny + b) * g.nz + c, j, C)]; };
+  double2 s = at(x1, y1, z1);
+  double2 t;
+  if (!xb) { t = at(xm, y1, z1); s.x -= t.x; s.y -= t.y; }
+  if (!yb) { t = at(x1, ym, z1); s.x -= t.x; s.y -= t.y; }
+  if (!zb) { t = at(x1, y1, zm); s.x -= t.x; s.y -= t.y; }
+  if (!xb && !yb) { t = at(xm, ym, z1); s.x += t.x; s.y += t.y; }
+  if (!xb && !zb) { t = at(xm, y1, zm); s.x += t.x; s.y += t.y; }
+  if (!yb && !zb) { t = at(x1, ym, zm); s.x += t.x; s.y += t.y; }
+  if (!xb && !yb && !zb) { t = at(xm, ym, zm); s.x -= t.x; s.y -= t.y; }
+  return s;
+}
+
+// Pass 4: thread = (cell, block, node j): shell difference x w x e^{+ik.c}.
+__global__ void k_gsat_shell(Grid g, GsatArgs a) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t j = (uint32_t)(t % kNodeBlock);
+  const size_t cb = t / kNodeBlock;
+  const uint32_t bb = (uint32_t)(cb % a.nblk);
+  const size_t c = cb / a.nblk;
+  if (c >= g.ncell) return;
+  const uint32_t k = (a.blk0 + bb) * kNodeBlock + j;
+  if (k >= a.K) return;
+  const uint32_t syz = g.ny * g.nz;
+  const uint32_t x = (uint32_t)(c / syz), rem = (uint32_t)(c - (size_t)x * syz);
+  const uint32_t y = rem / g.nz, z = rem - y * g.nz;
+  const uint32_t radii = a.node_radii[k];
+  const uint32_t r_out = radii >> 16, r_in = radii & 0xffffu;
+  const double w = a.node64[k].w;
+  const double2 o = gcube_sum(a.T, bb, j, x, y, z, r_out, g);
+  const double2 i = gcube_sum(a.T, bb, j, x, y, z, r_in, g);
+  const double2 sh = make_double2((o.x - i.x) * w, (o.y - i.y) * w);
+  const double2 *tk = a.tw + (size_t)k * (g.nx + g.ny + g.nz);
+  const double2 r = cmul(cmul(sh, tk[x]), cmul(tk[g.nx + y], tk[g.nx + g.ny + z]));
+  a.R[sr_index((uint32_t)c, k, g.ncell)] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
+}
+
+// ----------------------------------------------------------------------------
 // Long-range gather (src/glst_force.cu:983-1135 restated):
 //   en_i = q_i Re sum_k e^{ik.d_i} R'_c(k),   f_i = q_i sum_k Im(...) k
 // Nodes are held in the order group -> direction -> radial, k = kappa_r s_j,
@@ -693,8 +885,8 @@ __device__ __forceinline__ uint32_t cell_of_atom(const uint32_t *__restrict__ ce
 __global__ void __launch_bounds__(kLrThreads, 8)
 k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_point, uint32_t ncell,
                   const LrChunk *__restrict__ chunks, const float4 *__restrict__ dirs,
-                  const float *__restrict__ kappa, const float2 *__restrict__ R, uint32_t natom,
-                  double4 *__restrict__ part) {
+                  const float *__restrict__ kappa, const float2 *__restrict__ R, uint32_t node_off,
+                  uint32_t natom, int accumulate, double4 *__restrict__ part) {
   __shared__ float4 s_n[2][kLrfCells * kLrfSlot];
   __shared__ float4 s_kappa4[kLrfTilePairs / 2];
   __shared__ uint32_t s_range[2];
@@ -737,7 +929,7 @@ k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ ce
         const uint32_t dd = i / npr, r = 2 * (i - dd * npr);
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (c < nc && dd < nd) {
-          const uint32_t node = ch.node_begin + (d0 + dd) * nr + r;
+          const uint32_t node = ch.node_begin + (d0 + dd) * nr + r - node_off;
           const float2 x0 = R[sr_index(w0 + c, node, ncell)];
           const float2 x1 = (r + 1 < nr) ? R[sr_index(w0 + c, node + 1, ncell)] : make_float2(0.f, 0.f);
           v = make_float4(x0.x, x1.x, x0.y, x1.y);
@@ -833,7 +1025,13 @@ k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ ce
   }
   if (active) {
     const double q = static_cast<double>(pa.w);
-    part[(size_t)blockIdx.y * natom + p] = make_double4(q * ex, q * ey, q * ez, q * ee);
+    double4 *dst = part + (size_t)blockIdx.y * natom + p;
+    double4 v = make_double4(q * ex, q * ey, q * ez, q * ee);
+    if (accumulate) {  // a later node stage adds into the same rows
+      const double4 o = *dst;
+      v = make_double4(o.x + v.x, o.y + v.y, o.z + v.z, o.w + v.w);
+    }
+    *dst = v;
   }
 }
 
@@ -903,7 +1101,14 @@ k_short_range(const double4 *__restrict__ pd, const uint32_t *__restrict__ cell_
 // ----------------------------------------------------------------------------
 // Combine: near field + long-range partials (fixed order), write the
 // cell-ordered outputs and scatter to input order; per-CTA energy sums.
+// A CTA takes kCombineAtoms consecutive atoms; its warps split the partial
+// rows (warp w sums rows w, w + 8, ... for the warp's 32 atoms, each load a
+// coalesced 1 KB run), then warp 0 adds the eight row sums and the near-field
+// planes in a fixed order.  (One thread per atom summing every row left small
+// systems, with hundreds of rows and a few CTAs, latency-bound.)
 constexpr int kCombineThreads = 256;
+constexpr int kCombineAtoms = 32;
+constexpr int kCombineWarps = kCombineThreads / 32;
 
 __global__ void __launch_bounds__(kCombineThreads)
 k_combine(const double4 *__restrict__ sr, const double4 *__restrict__ part, uint32_t nsplit,
@@ -911,34 +1116,39 @@ k_combine(const double4 *__restrict__ sr, const double4 *__restrict__ part, uint
           double *__restrict__ cfx, double *__restrict__ cfy, double *__restrict__ cfz,
           double *__restrict__ cen, double *__restrict__ ofx, double *__restrict__ ofy,
           double *__restrict__ ofz, double *__restrict__ oen, double *__restrict__ block_energy) {
-  __shared__ double s_red[kCombineThreads / 32];
-  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ double4 s_rows[kCombineWarps][kCombineAtoms];
+  const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+  const uint32_t p = blockIdx.x * kCombineAtoms + lane;
+  const bool live = p < natom;
+  double4 acc = make_double4(0., 0., 0., 0.);
+  if (live && use_far) {
+    for (uint32_t s = w; s < nsplit; s += kCombineWarps) {
+      const double4 v = part[(size_t)s * natom + p];
+      acc.x += v.x; acc.y += v.y; acc.z += v.z; acc.w += v.w;
+    }
+  }
+  s_rows[w][lane] = acc;
+  __syncthreads();
+  if (w != 0) return;
   double e = 0.0;
-  if (p < natom) {
-    double4 acc = make_double4(0., 0., 0., 0.);
-    if (use_far) {
-      for (uint32_t s = 0; s < nsplit; s++) {
-        const double4 v = part[(size_t)s * natom + p];
-        acc.x += v.x; acc.y += v.y; acc.z += v.z; acc.w += v.w;
-      }
+  if (live) {
+    double4 t = s_rows[0][lane];
+#pragma unroll
+    for (int k = 1; k < kCombineWarps; k++) {
+      const double4 v = s_rows[k][lane];
+      t.x += v.x; t.y += v.y; t.z += v.z; t.w += v.w;
     }
     for (int pl = 0; pl < kSrPlanes; pl++) {
       const double4 v = sr[(size_t)pl * natom + p];
-      acc.x += v.x; acc.y += v.y; acc.z += v.z; acc.w += v.w;
+      t.x += v.x; t.y += v.y; t.z += v.z; t.w += v.w;
     }
-    cfx[p] = acc.x; cfy[p] = acc.y; cfz[p] = acc.z; cen[p] = acc.w;
+    cfx[p] = t.x; cfy[p] = t.y; cfz[p] = t.z; cen[p] = t.w;
     const uint32_t i = sorted_idx[p];
-    if (i < natom) { ofx[i] = acc.x; ofy[i] = acc.y; ofz[i] = acc.z; oen[i] = acc.w; }
-    e = acc.w;
+    if (i < natom) { ofx[i] = t.x; ofy[i] = t.y; ofz[i] = t.z; oen[i] = t.w; }
+    e = t.w;
   }
   for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
-  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = e;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int w = 0; w < kCombineThreads / 32; w++) t += s_red[w];
-    block_energy[blockIdx.x] = t;
-  }
+  if (lane == 0) block_energy[blockIdx.x] = e;
 }
 
 // Total energy 0.5 * sum of the per-CTA sums, fixed order (one CTA).

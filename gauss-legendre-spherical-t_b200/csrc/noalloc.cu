@@ -41,8 +41,7 @@ constexpr uint32_t kMaxCells = GLST_NOALLOC_MAX_CELLS;
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr size_t kOffCount = 0;
 constexpr size_t kOffPoint = kOffCount + align256(4ull * kMaxCells);
-constexpr size_t kOffFlags = kOffPoint + align256(4ull * kMaxCells);
-constexpr size_t kOffCell = kOffFlags + 256;
+constexpr size_t kOffCell = kOffPoint + align256(4ull * kMaxCells);
 constexpr size_t kOffSlot = kOffCell + align256(4ull * kMaxAtoms);
 constexpr size_t kOffPerm = kOffSlot + align256(4ull * kMaxAtoms);
 constexpr size_t kOffSorted = kOffPerm + align256(4ull * kMaxAtoms);
@@ -52,7 +51,7 @@ constexpr size_t kOffSr = kOffPd + align256(32ull * kMaxAtoms);
 constexpr size_t kOffCellOut = kOffSr + align256(32ull * kdev::kSrPlanes * kMaxAtoms);
 constexpr size_t kOffBlockE = kOffCellOut + align256(4ull * 8ull * kMaxAtoms);
 constexpr size_t kScratchBytes =
-    kOffBlockE + align256(8ull * ((kMaxAtoms + kdev::kCombineThreads - 1) / kdev::kCombineThreads));
+    kOffBlockE + align256(8ull * ((kMaxAtoms + kdev::kCombineAtoms - 1) / kdev::kCombineAtoms));
 static_assert(kScratchBytes == GLST_NOALLOC_SCRATCH_BYTES, "scratch size in glst_c.h is stale");
 
 // The scratch.  In host code `g_scratch` names a host-side stand-in, not
@@ -109,7 +108,20 @@ extern "C" glst_status glst_near_field_noalloc(uint32_t natom, const double *d_r
     return failed(GLST_ERR_INVALID_ARG);
   }
   // Cell grid in CT, as glst_create plans it (src/glst_force.cu:223-241).
+  // Each axis' cell count is checked against the limit before it is
+  // converted to an integer (a ratio beyond the range of `unsigned`, or not
+  // finite, would make the conversion undefined), so the product below
+  // cannot wrap either.
   const double box[3] = {box_x, box_y, box_z};
+  for (int a = 0; a < 3; a++) {
+    const double ratio = ct == GLST_CT_FLOAT ? static_cast<double>(static_cast<float>(box[a]) / static_cast<float>(rcut))
+                                             : box[a] / rcut;
+    if (!(ratio < static_cast<double>(kMaxCells))) {
+      std::snprintf(g_err, sizeof g_err, "box / rcut along axis %d exceeds the allocation-free limit of %u cells",
+                    a, kMaxCells);
+      return failed(GLST_ERR_SIZE);
+    }
+  }
   uint32_t n[3];
   double l;
   if (ct == GLST_CT_FLOAT) {
@@ -150,7 +162,6 @@ extern "C" glst_status glst_near_field_noalloc(uint32_t natom, const double *d_r
   const dev::Grid g{n[0], n[1], n[2], (uint32_t)ncell, l, ct == GLST_CT_FLOAT ? 1 : 0};
   uint32_t *cell_count = reinterpret_cast<uint32_t *>(base + kOffCount);
   uint32_t *cell_point = reinterpret_cast<uint32_t *>(base + kOffPoint);
-  uint32_t *flags = reinterpret_cast<uint32_t *>(base + kOffFlags);
   uint32_t *atom_cell = reinterpret_cast<uint32_t *>(base + kOffCell);
   uint32_t *atom_slot = reinterpret_cast<uint32_t *>(base + kOffSlot);
   uint32_t *perm = reinterpret_cast<uint32_t *>(base + kOffPerm);
@@ -161,22 +172,22 @@ extern "C" glst_status glst_near_field_noalloc(uint32_t natom, const double *d_r
   double *cell_out = reinterpret_cast<double *>(base + kOffCellOut);
   double *block_e = reinterpret_cast<double *>(base + kOffBlockE);
 
-  // The array keeps the previous call's contents: counts and flags restart at 0.
-  if ((e = cudaMemsetAsync(cell_count, 0, 4ull * ncell, st)) != cudaSuccess ||
-      (e = cudaMemsetAsync(flags, 0, 16, st)) != cudaSuccess) {
+  // The array keeps the previous call's contents: the cell counts restart at
+  // 0 (everything else is written before it is read).
+  if ((e = cudaMemsetAsync(cell_count, 0, 4ull * ncell, st)) != cudaSuccess) {
     std::snprintf(g_err, sizeof g_err, "cudaMemsetAsync failed: %s", cudaGetErrorString(e));
     return failed(GLST_ERR_CUDA);
   }
   if (natom) {
     const uint32_t nb = (natom + 255) / 256;
     dev::k_bin<<<nb, 256, 0, st>>>(d_rx, d_ry, d_rz, natom, g, atom_cell, atom_slot, cell_count);
-    dev::k_scan<<<1, 1024, 0, st>>>(cell_count, (uint32_t)ncell, cell_point, flags);
+    dev::k_scan<<<1, 1024, 0, st>>>(cell_count, (uint32_t)ncell, cell_point);
     dev::k_scatter<<<nb, 256, 0, st>>>(atom_cell, atom_slot, cell_point, natom, perm);
     dev::k_sort_pack<<<(uint32_t)ncell, 256, dev::kSortCap * sizeof(uint32_t), st>>>(
-        perm, cell_count, cell_point, g, d_rx, d_ry, d_rz, d_qc, sorted, pk, pd);
+        perm, cell_count, cell_point, g, atom_cell, natom, d_rx, d_ry, d_rz, d_qc, sorted, pk, pd);
     dev::k_short_range<<<dim3((uint32_t)ncell, dev::kSrPlanes), dev::kSrThreads, 0, st>>>(
         pd, cell_count, cell_point, g, natom, sr);
-    dev::k_combine<<<(natom + dev::kCombineThreads - 1) / dev::kCombineThreads, dev::kCombineThreads, 0, st>>>(
+    dev::k_combine<<<(natom + dev::kCombineAtoms - 1) / dev::kCombineAtoms, dev::kCombineThreads, 0, st>>>(
         sr, nullptr, 0, sorted, natom, 0, cell_out, cell_out + kMaxAtoms, cell_out + 2ull * kMaxAtoms,
         cell_out + 3ull * kMaxAtoms, d_fx, d_fy, d_fz, d_en, block_e);
     if ((e = cudaGetLastError()) != cudaSuccess) {

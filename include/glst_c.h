@@ -72,6 +72,13 @@ typedef struct glst_info {
   uint32_t group_r_out[16];
   uint64_t device_bytes;    /* device memory held by the handle */
   uint32_t kernels_per_compute; /* kernel launches of one glst_compute */
+  uint32_t node_stages;     /* far-field node stages of one compute: the
+                               structure factors and shell sums of a stage's
+                               nodes are held at a time (large systems hold a
+                               fraction of the ncell x K operand) */
+  uint32_t shell_sums_global; /* 1: the grid's per-node prefix table does not
+                               fit in shared memory; shell sums build their
+                               tables in global memory (any grid size) */
 } glst_info;
 
 /* Where spherical t-designs are read from.  Either the project's binary store
@@ -124,7 +131,10 @@ glst_status glst_compute(glst_handle *h, const double *d_rx, const double *d_ry,
 
 /* The six phases of calc_ener_force, for callers of the reference's phase
  * methods (include/glst_force.hcu:52-58).  Run in this order they produce
- * exactly what glst_compute produces. */
+ * exactly what glst_compute produces.  When the far field runs in several
+ * node stages (glst_info.node_stages > 1; the structure factors and shell
+ * sums of one stage are held at a time), glst_calc_sf runs the whole far
+ * field stage by stage and glst_sum_rmt_sf / glst_calc_lr_ef return at once. */
 glst_status glst_assign_atoms(glst_handle *h, const double *d_rx,
                               const double *d_ry, const double *d_rz,
                               const double *d_qc, void *stream); /* :431-534 */
@@ -210,12 +220,29 @@ glst_status glst_direct_coulomb(uint32_t natom, const double *d_rx,
  * dependent-chain loop over every SM.  Waits for the device. */
 glst_status glst_measure_pipe_peaks(double *sfu_per_s, double *fma_per_s);
 
-/* Device-side error flags raised by the last compute (bit 0: a cell held more
- * atoms than this build's per-cell limit).  Waits for the stream. */
+/* Device-side error flags raised by the last compute (none are raised by
+ * this build's kernels; GLST_ERR_STATE if any is set).  Waits for the stream. */
 glst_status glst_check(glst_handle *h, void *stream);
 
-/* Per-cell atom limit of this build (the cell sort runs in shared memory). */
+/* Atoms per cell the shared-memory cell sort holds.  Larger cells are
+ * ordered by a slower pass over all atoms; the assignment stays identical to
+ * the reference's (stable order by input index) at any cell size. */
 uint32_t glst_max_atoms_per_cell(void);
+
+/* Structure factors and shell sums of the positions last assigned (by
+ * glst_compute or glst_assign_atoms), recomputed stage by stage and returned
+ * in the reference's layout and definitions: host arrays of ncell x K
+ * doubles, row = cell, nodes in the reference's order (glst_get_nodes);
+ * sf = sum_j q_j e^{-i k.r_j} (the reference's sf_re_/sf_im_ after calc_sf,
+ * src/glst_force.cu:601-664) and rmt = w_k times the shell sum (its
+ * rmt_sum_re_/rmt_sum_im_ after sum_rmt_sf, :774-913).  This engine stores
+ * them cell-relative and pre-twiddled in FP32; the conversion is FP64 on the
+ * host.  For checking the two far-field phases separately; whole-system
+ * handles only (not shards).  Any pointer may be NULL; waits for the stream.
+ * No counterpart in the reference's public interface (the arrays are private
+ * members there). */
+glst_status glst_get_far_field(glst_handle *h, double *sf_re, double *sf_im,
+                               double *rmt_re, double *rmt_im, void *stream);
 
 /* ---------------------------------------------------------------------------
  * Batches: many independent systems solved together.  No counterpart in the
@@ -313,11 +340,11 @@ glst_status glst_server_get_stats(glst_server *s, glst_server_stats *st);
  * current); make that first call before any stream capture.  All calls share
  * the array: calls that overlap on the GPU (different streams or devices'
  * threads racing on one device) corrupt each other; serialise them.  Stream
- * ordered, does not wait for the GPU.  Cells above the per-cell sort limit
- * give correct forces in a non-reference within-cell order. */
+ * ordered, does not wait for the GPU.  The cell assignment is the
+ * reference's at any cell size. */
 #define GLST_NOALLOC_MAX_ATOMS 32768u
 #define GLST_NOALLOC_MAX_CELLS 32768u
-#define GLST_NOALLOC_SCRATCH_BYTES 6554880ull
+#define GLST_NOALLOC_SCRATCH_BYTES 6561792ull
 glst_status glst_near_field_noalloc(uint32_t natom, const double *d_rx,
                                     const double *d_ry, const double *d_rz,
                                     const double *d_qc, double box_x,

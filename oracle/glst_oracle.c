@@ -16,7 +16,10 @@
  *   SR          src/glst_force.cu:1248-1324 (own cell) and :1436-1544 (26 nbrs)
  *   direct sum  utils/coulomb.cu:14-82 (all pairs, open boundary)
  * Outputs are returned in input order (what get_ef gives, src/glst_force.cu:142-176).
+ * oracle_far_arrays returns the two far-field phases' arrays themselves (the
+ * reference's sf_re_/sf_im_ and rmt_sum_re_/rmt_sum_im_), for per-phase checks.
  */
+#define _GNU_SOURCE /* sincos */
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -114,6 +117,117 @@ static void cube_sum(double *re, double *im, const double *Pre, const double *Pi
   box_sum(re, im, Pre, Pim, x0, y0, z0, x1, y1, z1, ny, nz, k, K);
 }
 
+/* Structure factors (src/glst_force.cu:601-664) of cell-ordered atoms X over
+ * nodes [k0, k0 + K) into S[c * K + kk], then -- if R is non-NULL -- the
+ * inclusive prefix sums z, y, x (:702-772) in place and the shell sums times
+ * weight (:774-913) into R.  S_copy (may be NULL) receives S before the
+ * prefix sums. */
+static void far_arrays(const double *X, const uint32_t *cnt, const uint32_t *pnt, const oracle_plan *p,
+                       uint32_t k0, size_t K, double *Sre, double *Sim, double *Rre, double *Rim,
+                       double *S_copy_re, double *S_copy_im) {
+  const uint32_t nx = p->nx, ny = p->ny, nz = p->nz;
+  const uint32_t ncell = nx * ny * nz;
+  /* structure factors */
+#pragma omp parallel for schedule(dynamic, 1)
+  for (uint32_t c = 0; c < ncell; c++) {
+    for (size_t kk = 0; kk < K; kk++) {
+      const double kx = p->kx[k0 + kk], ky = p->ky[k0 + kk], kz = p->kz[k0 + kk];
+      double sr = 0.0, si = 0.0;
+      for (uint32_t a = pnt[c]; a < pnt[c] + cnt[c]; a++) {
+        double th = kx * X[4 * a] + ky * X[4 * a + 1] + kz * X[4 * a + 2];
+        double sn, cs;
+        sincos(th, &sn, &cs);
+        sr += X[4 * a + 3] * cs;
+        si -= X[4 * a + 3] * sn;
+      }
+      Sre[(size_t)c * K + kk] = sr;
+      Sim[(size_t)c * K + kk] = si;
+    }
+  }
+  if (S_copy_re) memcpy(S_copy_re, Sre, sizeof(double) * ncell * K);
+  if (S_copy_im) memcpy(S_copy_im, Sim, sizeof(double) * ncell * K);
+  if (!Rre || !Rim) return;
+  /* inclusive prefix sums: z, then y, then x */
+#pragma omp parallel for schedule(static)
+  for (size_t kk = 0; kk < K; kk++) {
+    for (uint32_t x = 0; x < nx; x++)
+      for (uint32_t y = 0; y < ny; y++) {
+        double ar = 0.0, ai = 0.0;
+        for (uint32_t z = 0; z < nz; z++) {
+          size_t o = ((size_t)(x * ny + y) * nz + z) * K + kk;
+          ar += Sre[o]; ai += Sim[o]; Sre[o] = ar; Sim[o] = ai;
+        }
+      }
+    for (uint32_t x = 0; x < nx; x++)
+      for (uint32_t z = 0; z < nz; z++) {
+        double ar = 0.0, ai = 0.0;
+        for (uint32_t y = 0; y < ny; y++) {
+          size_t o = ((size_t)(x * ny + y) * nz + z) * K + kk;
+          ar += Sre[o]; ai += Sim[o]; Sre[o] = ar; Sim[o] = ai;
+        }
+      }
+    for (uint32_t y = 0; y < ny; y++)
+      for (uint32_t z = 0; z < nz; z++) {
+        double ar = 0.0, ai = 0.0;
+        for (uint32_t x = 0; x < nx; x++) {
+          size_t o = ((size_t)(x * ny + y) * nz + z) * K + kk;
+          ar += Sre[o]; ai += Sim[o]; Sre[o] = ar; Sim[o] = ai;
+        }
+      }
+  }
+  /* shell sums times weight */
+#pragma omp parallel for schedule(static)
+  for (uint32_t c = 0; c < ncell; c++) {
+    uint32_t x = c / (ny * nz), y = (c / nz) % ny, z = c % nz;
+    for (size_t kk = 0; kk < K; kk++) {
+      uint32_t g = p->group[k0 + kk];
+      double orr, oi, ir, ii;
+      cube_sum(&orr, &oi, Sre, Sim, x, y, z, p->r_out[g], nx, ny, nz, kk, K);
+      cube_sum(&ir, &ii, Sre, Sim, x, y, z, p->r_in[g], nx, ny, nz, kk, K);
+      Rre[(size_t)c * K + kk] = (orr - ir) * p->w[k0 + kk];
+      Rim[(size_t)c * K + kk] = (oi - ii) * p->w[k0 + kk];
+    }
+  }
+}
+
+/* Cell assignment plus the cell-ordered packet array X (x, y, z, q). */
+static int assign_pack(uint32_t natom, const double *rx, const double *ry, const double *rz, const double *qc,
+                       const oracle_plan *p, uint32_t *atom_cell, uint32_t *cnt, uint32_t *pnt, uint32_t *sidx,
+                       double *X) {
+  if (oracle_assign(natom, rx, ry, rz, p, atom_cell, cnt, pnt, sidx) != 0) return -1;
+  for (uint32_t a = 0; a < natom; a++) {
+    uint32_t i = sidx[a];
+    X[4 * a + 0] = rx[i];
+    X[4 * a + 1] = ry[i];
+    X[4 * a + 2] = rz[i];
+    X[4 * a + 3] = qc[i];
+  }
+  return 0;
+}
+
+/* The reference's per-phase far-field arrays for all nodes: sf (after
+ * calc_sf) and rmt_sum (after sum_rmt_sf), [ncell][K] each, row = cell. */
+int oracle_far_arrays(uint32_t natom, const double *rx, const double *ry, const double *rz, const double *qc,
+                      const oracle_plan *p, double *sf_re, double *sf_im, double *rmt_re, double *rmt_im) {
+  const uint32_t ncell = p->nx * p->ny * p->nz;
+  const size_t K = p->K;
+  uint32_t *atom_cell = malloc(sizeof(uint32_t) * (natom ? natom : 1));
+  uint32_t *cnt = malloc(sizeof(uint32_t) * ncell);
+  uint32_t *pnt = malloc(sizeof(uint32_t) * ncell);
+  uint32_t *sidx = malloc(sizeof(uint32_t) * (natom ? natom : 1));
+  double *X = malloc(sizeof(double) * (natom ? natom : 1) * 4);
+  double *Sre = malloc(sizeof(double) * ncell * (K ? K : 1));
+  double *Sim = malloc(sizeof(double) * ncell * (K ? K : 1));
+  int rc = -1;
+  if (atom_cell && cnt && pnt && sidx && X && Sre && Sim &&
+      assign_pack(natom, rx, ry, rz, qc, p, atom_cell, cnt, pnt, sidx, X) == 0) {
+    far_arrays(X, cnt, pnt, p, 0, K, Sre, Sim, rmt_re, rmt_im, sf_re, sf_im);
+    rc = 0;
+  }
+  free(atom_cell); free(cnt); free(pnt); free(sidx); free(X); free(Sre); free(Sim);
+  return rc;
+}
+
 /* Far field (SF -> prefix sums -> shell sums -> LR) over nodes [k0, k1), plus
  * (if do_sr) the near field.  Accumulates into cell-ordered outputs, like the
  * reference's += into fx_/fy_/fz_/en_; returned in input order. */
@@ -130,14 +244,7 @@ int oracle_glst(uint32_t natom, const double *rx, const double *ry,
   double *X = malloc(sizeof(double) * (natom ? natom : 1) * 4);
   double *F = calloc((size_t)(natom ? natom : 1) * 4, sizeof(double));
   if (!atom_cell || !cnt || !pnt || !sidx || !X || !F) return -1;
-  oracle_assign(natom, rx, ry, rz, p, atom_cell, cnt, pnt, sidx);
-  for (uint32_t a = 0; a < natom; a++) {
-    uint32_t i = sidx[a];
-    X[4 * a + 0] = rx[i];
-    X[4 * a + 1] = ry[i];
-    X[4 * a + 2] = rz[i];
-    X[4 * a + 3] = qc[i];
-  }
+  assign_pack(natom, rx, ry, rz, qc, p, atom_cell, cnt, pnt, sidx, X);
   if (k1 > p->K) k1 = p->K;
   if (k0 > k1) k0 = k1;
   const size_t K = (size_t)(k1 - k0);
@@ -147,62 +254,7 @@ int oracle_glst(uint32_t natom, const double *rx, const double *ry,
     double *Rre = malloc(sizeof(double) * ncell * K);
     double *Rim = malloc(sizeof(double) * ncell * K);
     if (!Sre || !Sim || !Rre || !Rim) return -1;
-    /* structure factors */
-#pragma omp parallel for schedule(dynamic, 1)
-    for (uint32_t c = 0; c < ncell; c++) {
-      for (size_t kk = 0; kk < K; kk++) {
-        const double kx = p->kx[k0 + kk], ky = p->ky[k0 + kk], kz = p->kz[k0 + kk];
-        double sr = 0.0, si = 0.0;
-        for (uint32_t a = pnt[c]; a < pnt[c] + cnt[c]; a++) {
-          double th = kx * X[4 * a] + ky * X[4 * a + 1] + kz * X[4 * a + 2];
-          sr += X[4 * a + 3] * cos(th);
-          si -= X[4 * a + 3] * sin(th);
-        }
-        Sre[(size_t)c * K + kk] = sr;
-        Sim[(size_t)c * K + kk] = si;
-      }
-    }
-    /* inclusive prefix sums: z, then y, then x */
-#pragma omp parallel for schedule(static)
-    for (size_t kk = 0; kk < K; kk++) {
-      for (uint32_t x = 0; x < nx; x++)
-        for (uint32_t y = 0; y < ny; y++) {
-          double ar = 0.0, ai = 0.0;
-          for (uint32_t z = 0; z < nz; z++) {
-            size_t o = ((size_t)(x * ny + y) * nz + z) * K + kk;
-            ar += Sre[o]; ai += Sim[o]; Sre[o] = ar; Sim[o] = ai;
-          }
-        }
-      for (uint32_t x = 0; x < nx; x++)
-        for (uint32_t z = 0; z < nz; z++) {
-          double ar = 0.0, ai = 0.0;
-          for (uint32_t y = 0; y < ny; y++) {
-            size_t o = ((size_t)(x * ny + y) * nz + z) * K + kk;
-            ar += Sre[o]; ai += Sim[o]; Sre[o] = ar; Sim[o] = ai;
-          }
-        }
-      for (uint32_t y = 0; y < ny; y++)
-        for (uint32_t z = 0; z < nz; z++) {
-          double ar = 0.0, ai = 0.0;
-          for (uint32_t x = 0; x < nx; x++) {
-            size_t o = ((size_t)(x * ny + y) * nz + z) * K + kk;
-            ar += Sre[o]; ai += Sim[o]; Sre[o] = ar; Sim[o] = ai;
-          }
-        }
-    }
-    /* shell sums times weight */
-#pragma omp parallel for schedule(static)
-    for (uint32_t c = 0; c < ncell; c++) {
-      uint32_t x = c / (ny * nz), y = (c / nz) % ny, z = c % nz;
-      for (size_t kk = 0; kk < K; kk++) {
-        uint32_t g = p->group[k0 + kk];
-        double orr, oi, ir, ii;
-        cube_sum(&orr, &oi, Sre, Sim, x, y, z, p->r_out[g], nx, ny, nz, kk, K);
-        cube_sum(&ir, &ii, Sre, Sim, x, y, z, p->r_in[g], nx, ny, nz, kk, K);
-        Rre[(size_t)c * K + kk] = (orr - ir) * p->w[k0 + kk];
-        Rim[(size_t)c * K + kk] = (oi - ii) * p->w[k0 + kk];
-      }
-    }
+    far_arrays(X, cnt, pnt, p, k0, K, Sre, Sim, Rre, Rim, NULL, NULL);
     /* long-range gather */
 #pragma omp parallel for schedule(dynamic, 16)
     for (uint32_t a = 0; a < natom; a++) {
@@ -212,7 +264,8 @@ int oracle_glst(uint32_t natom, const double *rx, const double *ry,
       for (size_t kk = 0; kk < K; kk++) {
         const double kx = p->kx[k0 + kk], ky = p->ky[k0 + kk], kz = p->kz[k0 + kk];
         double th = kx * xa + ky * ya + kz * za;
-        double re = cos(th), im = sin(th);
+        double re, im;
+        sincos(th, &im, &re);
         double rr = Rre[(size_t)c * K + kk], ri = Rim[(size_t)c * K + kk];
         double dre = qa * (re * rr - im * ri);
         double dim = qa * (re * ri + im * rr);

@@ -42,6 +42,7 @@ def lib():
         build()
         _lib = ctypes.CDLL(SO)
         _lib.oracle_glst.restype = ctypes.c_int
+        _lib.oracle_far_arrays.restype = ctypes.c_int
         _lib.oracle_assign.restype = ctypes.c_int
         _lib.oracle_num_threads.restype = ctypes.c_int
     return _lib
@@ -106,6 +107,23 @@ def glst(x, y, z, q, plan, k0=0, k1=None, far=True, sr=True):
     if rc != 0:
         raise MemoryError("oracle_glst failed")
     return tuple(out)
+
+
+def far_arrays(x, y, z, q, plan):
+    """The reference's per-phase far-field arrays (FP64), complex [ncell, K]:
+    sf = sum_j q_j e^{-ik.r_j} after calc_sf (src/glst_force.cu:601-664) and
+    rmt = w times the shell sum after sum_rmt_sf (:702-913)."""
+    n = len(x)
+    cp, keep = _cplan(plan)
+    x, y, z, q = _d(x), _d(y), _d(z), _d(q)
+    C, K = plan.ncell, plan.K
+    out = [np.empty((C, K)) for _ in range(4)]
+    V = ctypes.c_void_p
+    rc = lib().oracle_far_arrays(ctypes.c_uint32(n), x.ctypes.data_as(V), y.ctypes.data_as(V), z.ctypes.data_as(V),
+                                 q.ctypes.data_as(V), ctypes.byref(cp), *[o.ctypes.data_as(V) for o in out])
+    if rc != 0:
+        raise MemoryError("oracle_far_arrays failed")
+    return out[0] + 1j * out[1], out[2] + 1j * out[3]
 
 
 def coulomb(x, y, z, q):

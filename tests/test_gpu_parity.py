@@ -236,24 +236,6 @@ def test_atoms_outside_box_are_clamped(pkg, store):
     f.close()
 
 
-def test_dense_cell_overflow_is_reported(pkg):
-    """A cell with more atoms than the in-shared-memory sort holds: results
-    stay correct, glst_check reports GLST_ERR_SIZE."""
-    rng = np.random.default_rng(9)
-    n = 9000
-    pts = rng.uniform(0.5, 9.5, size=(n, 3))  # all in cell (0,0,0) of 2x2x2
-    q = rng.choice([-0.5, 0.5], n)
-    x, y, z = (np.ascontiguousarray(pts[:, i]) for i in range(3))
-    f, got = _run(pkg, x, y, z, q, 1e-4, 20.0, 10.0)
-    with pytest.raises(pkg.GlstError) as e:
-        f.check()
-    assert e.value.status == 7
-    ref = oracle.coulomb(x, y, z, q)
-    rep = oracle.error_report(got, ref)
-    assert rep["force_rms_rel"] <= 1e-11, rep
-    f.close()
-
-
 @pytest.mark.slow
 def test_water10k_parity(pkg, store):
     """water10k workload: 10,000 waters, L = 66.9 A, rcut 10, alpha 0.31."""

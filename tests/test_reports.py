@@ -3,7 +3,8 @@
 error_stats must be the statistics of utils/utils.cpp:60-125, and a log made
 by format_run_log must be read by the reference's own
 utils/parse_glst_results.py into the fields its CSV has (run only where the
-reference sources are present; the script is imported, not copied).
+environment variable REF_ROOT names the reference source tree; the script is
+imported, not copied).
 """
 import importlib.util
 import math
@@ -13,7 +14,7 @@ import types
 import numpy as np
 import pytest
 
-REF_PARSER = "/root/reference/utils/parse_glst_results.py"
+REF_PARSER = os.path.join(os.environ.get("REF_ROOT", ""), "utils", "parse_glst_results.py")
 
 
 def _info():
