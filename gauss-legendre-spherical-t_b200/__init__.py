@@ -82,6 +82,7 @@ _SIGNATURES = {
     "glst_get_nodes": (_I, [_P, _P, _P, _P, _P, _P]),
     "glst_check": (_I, [_P, _P]),
     "glst_get_far_field": (_I, [_P, _P, _P, _P, _P, _P]),
+    "glst_reduce_shards": (_I, [_P, _U32, _P]),
     "glst_plan": (_I, [_U32, _D, _D, _D, _D, _D, _I, ctypes.POINTER(GlstInfo), _P, _P, _P, _P, _P]),
     "glst_max_atoms_per_cell": (_U32, []),
     "glst_measure_pipe_peaks": (_I, [_DP, _DP]),
@@ -337,6 +338,18 @@ class GlstForce:
         arrs = [np.empty(K) for _ in range(4)] + [np.empty(K, dtype=np.uint32)]
         _check(self._lib.glst_get_nodes(self._h, *[a.ctypes.data for a in arrs]))
         return tuple(arrs)
+
+
+def reduce_shards(shards, streams=None):
+    """Sum the outputs of shard handles 0..n-1 of one system into shard 0's
+    (glst_reduce_shards: the reference's reduce to the first GPU).  shards:
+    GlstForce objects made with shard=(s, n), each computed on streams[s]
+    (default: the legacy stream)."""
+    lib = load_library()
+    n = len(shards)
+    hs = (ctypes.c_void_p * n)(*[s._h.value for s in shards])
+    sts = (ctypes.c_void_p * n)(*[_stream(s) for s in (streams or [None] * n)])
+    _check(lib.glst_reduce_shards(hs, n, sts))
 
 
 class GlstBatch:

@@ -616,10 +616,11 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
     int smem_optin = 0, nsm = 148;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
     CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
-    // row stride = 1 (mod 8) complex doubles: rows of consecutive nodes start
-    // 16 bytes apart modulo 128, so the node-fastest accesses of the shell
-    // pass spread over all shared-memory banks
-    h->sat_stride = (uint32_t)(C + 1);
+    // row = a node's prefix table with a zero plane in front along each
+    // axis; row stride = 1 (mod 8) complex doubles: rows of consecutive nodes
+    // start 16 bytes apart modulo 128, so the node-fastest accesses of the
+    // shell pass spread over all shared-memory banks
+    h->sat_stride = dev::sat_padded_cells(p.n[0], p.n[1], p.n[2]);
     while (h->sat_stride % 8 != 1) h->sat_stride++;
     const size_t per_node = ((size_t)h->sat_stride + p.n[0] + p.n[1] + p.n[2]) * sizeof(double2);
     // the cell-coordinate table (4 bytes per cell) comes off the budget when
@@ -1279,6 +1280,62 @@ glst_status glst_check(glst_handle *h, void *stream) {
   CUDA_TRY(cudaMemcpyAsync(flags, h->flags, sizeof flags, cudaMemcpyDeviceToHost, S_(stream)));
   CUDA_TRY(cudaStreamSynchronize(S_(stream)));
   if (flags[0]) return fail(GLST_ERR_STATE, "device error flags 0x%x raised by the last compute", flags[0]);
+  return GLST_OK;
+}
+
+glst_status glst_reduce_shards(glst_handle *const *shards, uint32_t n, void *const *streams) {
+  if (!shards || !streams || n == 0) return fail(GLST_ERR_INVALID_ARG, "null argument or no shards");
+  if (n > (uint32_t)dev::kMaxShards) return fail(GLST_ERR_SIZE, "at most %d shards", dev::kMaxShards);
+  glst_handle *h0 = shards[0];
+  for (uint32_t s = 0; s < n; s++) {
+    const glst_handle *h = shards[s];
+    if (!h) return fail(GLST_ERR_INVALID_ARG, "null shard handle");
+    if (h->nshards != n || h->shard != s)
+      return fail(GLST_ERR_INVALID_ARG, "shards[%u] is shard %u of %u, expected %u of %u", s, h->shard, h->nshards, s,
+                  n);
+    if (h->plan.natom != h0->plan.natom || h->plan.ncell != h0->plan.ncell)
+      return fail(GLST_ERR_INVALID_ARG, "shards of different systems");
+    if (!h->computed) return fail(GLST_ERR_STATE, "shard %u has not computed", s);
+  }
+  if (n == 1) return GLST_OK;
+  const uint32_t N = h0->plan.natom;
+  DeviceGuard guard_(h0);
+  cudaStream_t st0 = S_(streams[0]);
+  // shard 0's stream waits for every other shard's compute; peer access from
+  // shard 0's device to theirs
+  for (uint32_t s = 1; s < n; s++) {
+    glst_handle *h = shards[s];
+    if (h->device != h0->device) {
+      int ok = 0;
+      CUDA_TRY(cudaDeviceCanAccessPeer(&ok, h0->device, h->device));
+      if (!ok) return fail(GLST_ERR_CUDA, "device %d cannot access device %d's memory", h0->device, h->device);
+      const cudaError_t e = cudaDeviceEnablePeerAccess(h->device, 0);
+      if (e == cudaErrorPeerAccessAlreadyEnabled) cudaGetLastError();
+      else if (e != cudaSuccess) return fail(GLST_ERR_CUDA, "peer access: %s", cudaGetErrorString(e));
+      CUDA_TRY(cudaSetDevice(h->device));
+    }
+    // ev_join of shard s: recorded on its own compute stream, on its device
+    CUDA_TRY(cudaEventRecord(h->ev_join, S_(streams[s])));
+    if (h->device != h0->device) CUDA_TRY(cudaSetDevice(h0->device));
+    CUDA_TRY(cudaStreamWaitEvent(st0, h->ev_join, 0));
+  }
+  if (!N) return GLST_OK;
+  dev::ShardSet ss{};
+  ss.n = n;
+  for (uint32_t s = 0; s < n; s++) {
+    const glst_handle *h = shards[s];
+    const double *a[8] = {h->ofx, h->ofy, h->ofz, h->oen, h->cfx, h->cfy, h->cfz, h->cen};
+    for (int k = 0; k < 8; k++) ss.src[s][k] = a[k];
+  }
+  // the sums land in shard 0's outputs: every element is read from all
+  // shards before it is written (one thread per element)
+  double *d[8] = {h0->ofx, h0->ofy, h0->ofz, h0->oen, h0->cfx, h0->cfy, h0->cfz, h0->cen};
+  for (int k = 0; k < 8; k++) ss.dst[k] = d[k];
+  const uint32_t nb = (N + dev::kCombineThreads - 1) / dev::kCombineThreads;  // <= combine_blocks
+  dev::k_reduce_shards<<<nb, dev::kCombineThreads, 0, st0>>>(ss, N, h0->block_energy);
+  CUDA_TRY(cudaGetLastError());
+  dev::k_energy_total<<<1, 256, 0, st0>>>(h0->block_energy, nb, h0->energy);
+  CUDA_TRY(cudaGetLastError());
   return GLST_OK;
 }
 

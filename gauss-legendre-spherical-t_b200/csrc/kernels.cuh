@@ -473,7 +473,13 @@ k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ 
 // R_c = w * [box(c, r_out) - box(c, r_in)], 8 corners per box, clipped to the
 // grid.  All FP64.  Output R'_c(k) = R_c(k) e^{+ik.c} as float2, the twiddle
 // built from per-axis tables e^{i kx cx} e^{i ky cy} e^{i kz cz}.
-// CTA: nb nodes at once (rows of ncell+1 complex doubles in shared memory).
+// The prefix table of a node is held with one zero plane in front along
+// every axis ((nx+1) x (ny+1) x (nz+1) entries, entry (X, Y, Z) = sum over
+// cells x < X, y < Y, z < Z): a box corner that falls outside the grid reads
+// a zero instead of being skipped, so every box is eight unconditional loads
+// at offsets X*sx + Y*sy + Z built from two values per axis.  (Adding or
+// subtracting an exact zero leaves the result bit for bit as the clipped sum.)
+// CTA: nb nodes at once (rows of `stride` complex doubles in shared memory).
 constexpr int kSatThreads = 512;
 constexpr int kSatThreadsOne = 1024;  // one node per CTA (large grids): more warps per SM
 constexpr int kSatLoadBatch = 4;
@@ -487,39 +493,41 @@ struct SatArgs {
   uint32_t nb;                  // nodes per CTA (a power of two, <= 32)
   uint32_t lg_nb;               // log2(nb)
   uint32_t xyz_table;           // 1: cell coordinates tabulated in shared memory
-  uint32_t stride;              // shared row stride (complex), >= ncell, = 1 (mod 8)
+  uint32_t stride;              // shared row stride (complex), >= padded table size, = 1 (mod 8)
   float2 *R;
 };
 
-__device__ __forceinline__ double2 sat_at(const double2 *row, uint32_t x, uint32_t y,
-                                          uint32_t z, const Grid &g) {
-  return row[(x * g.ny + y) * g.nz + z];
-}
-
-__device__ __forceinline__ double2 cube_sum(const double2 *row, uint32_t x, uint32_t y,
-                                            uint32_t z, uint32_t r, const Grid &g) {
-  const uint32_t x0 = (x < r) ? 0 : x - r, y0 = (y < r) ? 0 : y - r, z0 = (z < r) ? 0 : z - r;
-  const uint32_t x1 = min(x + r, g.nx - 1), y1 = min(y + r, g.ny - 1), z1 = min(z + r, g.nz - 1);
-  const bool xb = x0 == 0, yb = y0 == 0, zb = z0 == 0;
-  const uint32_t xm = xb ? 0 : x0 - 1, ym = yb ? 0 : y0 - 1, zm = zb ? 0 : z0 - 1;
-  double2 s = sat_at(row, x1, y1, z1, g);
-  double2 t;
-  if (!xb) { t = sat_at(row, xm, y1, z1, g); s.x -= t.x; s.y -= t.y; }
-  if (!yb) { t = sat_at(row, x1, ym, z1, g); s.x -= t.x; s.y -= t.y; }
-  if (!zb) { t = sat_at(row, x1, y1, zm, g); s.x -= t.x; s.y -= t.y; }
-  if (!xb && !yb) { t = sat_at(row, xm, ym, z1, g); s.x += t.x; s.y += t.y; }
-  if (!xb && !zb) { t = sat_at(row, xm, y1, zm, g); s.x += t.x; s.y += t.y; }
-  if (!yb && !zb) { t = sat_at(row, x1, ym, zm, g); s.x += t.x; s.y += t.y; }
-  if (!xb && !yb && !zb) { t = sat_at(row, xm, ym, zm, g); s.x -= t.x; s.y -= t.y; }
-  return s;
+// Entries of a node's padded prefix table.
+__host__ __device__ __forceinline__ uint32_t sat_padded_cells(uint32_t nx, uint32_t ny, uint32_t nz) {
+  return (nx + 1) * (ny + 1) * (nz + 1);
 }
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// Dynamic shared memory: nb rows of `stride` complex (the SAT), the twiddle
-// tables nb x (nx + ny + nz) complex, then, in the several-nodes form
+// Box sum of the cells [x0, x1] x [y0, y1] x [z0, z1] from the padded table:
+// the caller passes the corner coordinates already scaled by the strides:
+// xl = x0 * sx, xh = (x1 + 1) * sx, likewise y with sy, z unscaled.  The eight
+// terms are added in the order of the reference's box_sum
+// (src/glst_force.cu:774-845).
+__device__ __forceinline__ double2 box_padded(const double2 *row, uint32_t xl, uint32_t xh, uint32_t yl,
+                                              uint32_t yh, uint32_t zl, uint32_t zh) {
+  const uint32_t hh = xh + yh, lh = xl + yh, hl = xh + yl, ll = xl + yl;
+  double2 s = row[hh + zh];
+  double2 t;
+  t = row[lh + zh]; s.x -= t.x; s.y -= t.y;
+  t = row[hl + zh]; s.x -= t.x; s.y -= t.y;
+  t = row[hh + zl]; s.x -= t.x; s.y -= t.y;
+  t = row[ll + zh]; s.x += t.x; s.y += t.y;
+  t = row[lh + zl]; s.x += t.x; s.y += t.y;
+  t = row[hl + zl]; s.x += t.x; s.y += t.y;
+  t = row[ll + zl]; s.x -= t.x; s.y -= t.y;
+  return s;
+}
+
+// Dynamic shared memory: nb rows of `stride` complex (the padded tables), the
+// twiddle tables nb x (nx + ny + nz) complex, then, in the several-nodes form
 // (kMinBlocks > 1, small grids) when it fits, the cell coordinates (ncell x
 // u32, x | y << 10 | z << 20).  nb is a power of two <= 32: lane l of a warp works
 // on node l % nb of the CTA and on the (l / nb)-th of the 32 / nb cells or
@@ -534,6 +542,7 @@ k_shell_sums(Grid g, SatArgs a) {
   const uint32_t k0 = blockIdx.x * nb;
   const uint32_t C = g.ncell;
   const uint32_t naxis = g.nx + g.ny + g.nz;
+  const uint32_t sy = g.nz + 1, sx = (g.ny + 1) * sy;  // padded strides
   double2 *s_tw = s_sat + (size_t)nb * a.stride;
   uint32_t *s_xyz = reinterpret_cast<uint32_t *>(s_tw + (size_t)nb * naxis);
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -572,6 +581,22 @@ k_shell_sums(Grid g, SatArgs a) {
     sincos(kc, &sn, &cs);
     s_tw[t] = make_double2(cs, sn);
   }
+  // the zero planes X = 0 and Y = 0 of every row (the Z = 0 entries of the
+  // other lines are written by the load pass)
+  {
+    const uint32_t nxz = g.nx * sy;
+    for (uint32_t t = threadIdx.x; t < nb * (sx + nxz); t += blockDim.x) {
+      const uint32_t jj = t / (sx + nxz), r = t - jj * (sx + nxz);
+      uint32_t off;
+      if (r < sx) {
+        off = r;
+      } else {
+        const uint32_t q = r - sx, xq = q / sy;
+        off = (xq + 1) * sx + (q - xq * sy);
+      }
+      s_sat[(size_t)jj * a.stride + off] = zero;
+    }
+  }
   auto coords = [&](uint32_t c) {
     const uint32_t x = c / (g.ny * g.nz), rem = c - x * (g.ny * g.nz);
     const uint32_t y = rem / g.nz, z = rem - y * g.nz;
@@ -587,15 +612,17 @@ k_shell_sums(Grid g, SatArgs a) {
   // prefix pass without its own shared-memory round trip)
   {
     double2 acc = zero, txy = zero;
+    uint32_t base = 0;
     while (l < nlines) {
       uint32_t ln = l, zn = z0 + kSatLoadBatch;
       if (zn >= g.nz) { ln = l + step; zn = 0; }
       if (z0 == 0) {
-        const uint32_t lx = l / g.ny;
-        txy = cmul(twx[lx], twy[l - lx * g.ny]);  // e^{+i(kx cx + ky cy)}
+        const uint32_t lx = l / g.ny, ly = l - lx * g.ny;
+        txy = cmul(twx[lx], twy[ly]);  // e^{+i(kx cx + ky cy)}
         acc = zero;
+        base = (lx + 1) * sx + (ly + 1) * sy;  // padded line (x + 1, y + 1, .)
+        row[base] = zero;                      // its Z = 0 entry
       }
-      const uint32_t base = l * g.nz;
 #pragma unroll
       for (int u = 0; u < kSatLoadBatch; u++) {
         if (z0 + u < g.nz) {
@@ -603,7 +630,7 @@ k_shell_sums(Grid g, SatArgs a) {
           const double vx = v[u].x, vy = v[u].y;
           acc.x += vx * t.x + vy * t.y;  // v * conj(t)
           acc.y += vy * t.x - vx * t.y;
-          row[base + z0 + u] = acc;
+          row[base + z0 + u + 1] = acc;
         }
       }
       fetch(v, ln, zn);
@@ -615,19 +642,17 @@ k_shell_sums(Grid g, SatArgs a) {
   // prefix along y (lines x, z)
   for (uint32_t l = first; l < g.nx * g.nz; l += step) {
     const uint32_t x = l / g.nz, z = l - x * g.nz;
-    double2 *p = row + x * g.ny * g.nz + z;
-    double2 acc = make_double2(0.0, 0.0);
-    for (uint32_t y = 0; y < g.ny; y++) { acc.x += p[y * g.nz].x; acc.y += p[y * g.nz].y; p[y * g.nz] = acc; }
+    double2 *p = row + (x + 1) * sx + (z + 1);
+    double2 acc = zero;
+    for (uint32_t y = 1; y <= g.ny; y++) { acc.x += p[y * sy].x; acc.y += p[y * sy].y; p[y * sy] = acc; }
   }
   __syncthreads();
   // prefix along x (lines y, z)
-  {
-    const uint32_t sx = g.ny * g.nz;
-    for (uint32_t l = first; l < sx; l += step) {
-      double2 *p = row + l;
-      double2 acc = make_double2(0.0, 0.0);
-      for (uint32_t x = 0; x < g.nx; x++) { acc.x += p[x * sx].x; acc.y += p[x * sx].y; p[x * sx] = acc; }
-    }
+  for (uint32_t l = first; l < g.ny * g.nz; l += step) {
+    const uint32_t y = l / g.nz, z = l - y * g.nz;
+    double2 *p = row + (y + 1) * sy + (z + 1);
+    double2 acc = zero;
+    for (uint32_t x = 1; x <= g.nx; x++) { acc.x += p[x * sx].x; acc.y += p[x * sx].y; p[x * sx] = acc; }
   }
   __syncthreads();
   if (!jv) return;
@@ -635,6 +660,19 @@ k_shell_sums(Grid g, SatArgs a) {
   const uint32_t radii = a.node_radii[k];
   const uint32_t r_out = radii >> 16, r_in = radii & 0xffffu;
   const double w = a.node64[k].w;
+  auto shell = [&](uint32_t x, uint32_t y, uint32_t z) {
+    // padded corner coordinates of the outer and inner cube, per axis
+    const uint32_t xo0 = (x > r_out ? x - r_out : 0u) * sx, xo1 = (min(x + r_out, g.nx - 1) + 1) * sx;
+    const uint32_t yo0 = (y > r_out ? y - r_out : 0u) * sy, yo1 = (min(y + r_out, g.ny - 1) + 1) * sy;
+    const uint32_t zo0 = (z > r_out ? z - r_out : 0u), zo1 = min(z + r_out, g.nz - 1) + 1;
+    const uint32_t xi0 = (x > r_in ? x - r_in : 0u) * sx, xi1 = (min(x + r_in, g.nx - 1) + 1) * sx;
+    const uint32_t yi0 = (y > r_in ? y - r_in : 0u) * sy, yi1 = (min(y + r_in, g.ny - 1) + 1) * sy;
+    const uint32_t zi0 = (z > r_in ? z - r_in : 0u), zi1 = min(z + r_in, g.nz - 1) + 1;
+    const double2 o = box_padded(row, xo0, xo1, yo0, yo1, zo0, zo1);
+    const double2 i = box_padded(row, xi0, xi1, yi0, yi1, zi0, zi1);
+    const double2 sh = make_double2((o.x - i.x) * w, (o.y - i.y) * w);
+    return cmul(cmul(sh, twx[x]), cmul(twy[y], twz[z]));
+  };
   // The thread's cells c = first + i * step.  Small grids (several nodes per
   // CTA) look their coordinates up in the CTA's table.  Large grids (one node
   // per CTA) step them with carries: there the table cost every CTA two
@@ -644,28 +682,21 @@ k_shell_sums(Grid g, SatArgs a) {
   if constexpr (kMinBlocks > 1) {
     for (uint32_t c = first; c < C; c += step) {
       const uint32_t xyz = a.xyz_table ? s_xyz[c] : coords(c);
-      const uint32_t x = xyz & 1023u, y = (xyz >> 10) & 1023u, z = xyz >> 20;
-      const double2 o = cube_sum(row, x, y, z, r_out, g);
-      const double2 i = cube_sum(row, x, y, z, r_in, g);
-      const double2 sh = make_double2((o.x - i.x) * w, (o.y - i.y) * w);
-      const double2 r = cmul(cmul(sh, twx[x]), cmul(twy[y], twz[z]));
+      const double2 r = shell(xyz & 1023u, (xyz >> 10) & 1023u, xyz >> 20);
       a.R[sr_index(c, ks, C)] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
     }
   } else {
     const uint32_t syz = g.ny * g.nz;
-    const uint32_t sx = step / syz, sy = (step - sx * syz) / g.nz, sz = step - sx * syz - sy * g.nz;
+    const uint32_t dx = step / syz, dy = (step - dx * syz) / g.nz, dz = step - dx * syz - dy * g.nz;
     uint32_t x = first / syz, y = (first - x * syz) / g.nz, z = first - x * syz - y * g.nz;
     for (uint32_t c = first; c < C; c += step) {
-      const double2 o = cube_sum(row, x, y, z, r_out, g);
-      const double2 i = cube_sum(row, x, y, z, r_in, g);
-      const double2 sh = make_double2((o.x - i.x) * w, (o.y - i.y) * w);
-      const double2 r = cmul(cmul(sh, twx[x]), cmul(twy[y], twz[z]));
+      const double2 r = shell(x, y, z);
       a.R[sr_index(c, ks, C)] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
-      z += sz;  // sz < nz and sy < ny: one carry at most per axis
+      z += dz;  // dz < nz and dy < ny: one carry at most per axis
       if (z >= g.nz) { z -= g.nz; y++; }
-      y += sy;
+      y += dy;
       if (y >= g.ny) { y -= g.ny; x++; }
-      x += sx;
+      x += dx;
     }
   }
 }
@@ -1149,6 +1180,44 @@ k_combine(const double4 *__restrict__ sr, const double4 *__restrict__ part, uint
   }
   for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
   if (lane == 0) block_energy[blockIdx.x] = e;
+}
+
+// ----------------------------------------------------------------------------
+// Sum of the per-atom outputs of the node-range shards of one system (the
+// reference's reduce to GPU 0, src/glst_force.cu:1584-1602 with
+// src/device_comm.cu:176-201 ncclReduce): dst[i] = src[0][i] + src[1][i] +
+// ..., shards in order, for the four input-order and the four cell-order
+// arrays.  The sources may live on other GPUs (read over NVLink through peer
+// access).  Per-CTA energy sums as k_combine writes them.
+constexpr int kMaxShards = 16;
+struct ShardSet {
+  const double *src[kMaxShards][8];  // per shard: ofx, ofy, ofz, oen, cfx, cfy, cfz, cen
+  double *dst[8];
+  uint32_t n;
+};
+
+__global__ void __launch_bounds__(kCombineThreads)
+k_reduce_shards(ShardSet ss, uint32_t natom, double *__restrict__ block_energy) {
+  __shared__ double s_red[kCombineThreads / 32];
+  const uint32_t i = blockIdx.x * kCombineThreads + threadIdx.x;
+  double e = 0.0;
+  if (i < natom) {
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+      double t = 0.0;
+      for (uint32_t s = 0; s < ss.n; s++) t += ss.src[s][a][i];
+      ss.dst[a][i] = t;
+      if (a == 3) e = t;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = e;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kCombineThreads / 32; w++) t += s_red[w];
+    block_energy[blockIdx.x] = t;
+  }
 }
 
 // Total energy 0.5 * sum of the per-CTA sums, fixed order (one CTA).

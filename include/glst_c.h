@@ -115,6 +115,19 @@ glst_status glst_create_shard(glst_handle **out, uint32_t natom, double tol,
                               double rcut, glst_ct ct, uint32_t shard,
                               uint32_t nshards);
 
+/* The reference's reduction of the shards' partial results to the first GPU
+ * (comm_ef, src/glst_force.cu:1584-1602: ncclReduce of fx, fy, fz, en to
+ * device 0, src/device_comm.cu:176-201).  shards[s] is shard s of n of one
+ * system (glst_create_shard), each after its glst_compute on streams[s]
+ * (its own device).  Shard 0's device reads the other shards' outputs
+ * directly over NVLink (peer access, enabled here when the devices differ)
+ * and sums them in shard order into shard 0's outputs, input and cell order,
+ * and its total energy; glst_get_ef / glst_energy on shard 0 then return
+ * the whole system's result.  Stream ordered on streams[0], which first waits
+ * for every shard's stream.  At most 16 shards. */
+glst_status glst_reduce_shards(glst_handle *const *shards, uint32_t n,
+                               void *const *streams);
+
 /* glst_force::init(natom, tol, Lx, Ly, Lz, rcut)   src/glst_force.cu:179-327 */
 glst_status glst_init(glst_handle *h, uint32_t natom, double tol, double box_x,
                       double box_y, double box_z, double rcut);

@@ -14,6 +14,7 @@
 //
 // usage: glst_ref_harness <in.bin> <out.bin> <float|double> <iterations>
 //        glst_ref_harness --batch <list.bin> <out.bin> <float|double> <iterations>
+//                         [<forces.bin> <every>]
 //   in.bin : u32 natom, f64 tol, f64 box[3], f64 rcut, f64 x[N], y[N], z[N], q[N]
 //   out.bin: u32 natom, u32 K, u32 nx, ny, nz, u32 iterations,
 //            f64 ms_mean[8] (assign, sf, sum, lr, sr, comm, total, events_total),
@@ -125,8 +126,10 @@ static int run(const char *out_path, unsigned natom, double tol,
 //   list.bin: u32 nsys, then per system the in.bin record above
 //   out.bin : u32 nsys, then per system u32 natom, u32 K, f64 ms_host,
 //             f64 ms_events, f64 energy (0.5 * sum en)
+//   forces.bin (optional, with every > 0): for systems s with s % every == 0,
+//             u32 s, u32 natom, f64 fx[N], fy[N], fz[N], en[N] (input order)
 template <typename CT>
-static int run_batch(FILE *in, FILE *out, unsigned nsys, int iters) {
+static int run_batch(FILE *in, FILE *out, unsigned nsys, int iters, FILE *forces, unsigned every) {
   std::fwrite(&nsys, sizeof(unsigned), 1, out);
   for (unsigned s = 0; s < nsys; s++) {
     unsigned natom = 0;
@@ -178,6 +181,11 @@ static int run_batch(FILE *in, FILE *out, unsigned nsys, int iters) {
       glst.get_ef(fx, fy, fz, en);
       for (unsigned i = 0; i < natom; i++) energy += en.h_array()[i];
       energy *= 0.5;
+      if (forces && every && s % every == 0) {
+        std::fwrite(&s, sizeof(unsigned), 1, forces);
+        std::fwrite(&natom, sizeof(unsigned), 1, forces);
+        for (auto *c : {&fx, &fy, &fz, &en}) std::fwrite(c->h_array().data(), sizeof(double), natom, forces);
+      }
     }
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) {
@@ -197,24 +205,33 @@ static int run_batch(FILE *in, FILE *out, unsigned nsys, int iters) {
 }
 
 int main(int argc, char **argv) {
-  if (argc == 6 && std::string(argv[1]) == "--batch") {
+  // --batch list.bin out.bin float|double iterations [forces.bin every]
+  if ((argc == 6 || argc == 8) && std::string(argv[1]) == "--batch") {
     FILE *in = std::fopen(argv[2], "rb");
     if (!in) return 2;
     FILE *out = std::fopen(argv[3], "wb");
     if (!out) return 2;
+    FILE *forces = nullptr;
+    unsigned every = 0;
+    if (argc == 8) {
+      forces = std::fopen(argv[6], "wb");
+      if (!forces) return 2;
+      every = (unsigned)std::atoi(argv[7]);
+    }
     unsigned nsys = 0;
     if (std::fread(&nsys, sizeof(unsigned), 1, in) != 1) return 2;
     int rc = 0;
     try {
       rc = std::string(argv[4]) == "float"
-               ? run_batch<float>(in, out, nsys, std::atoi(argv[5]))
-               : run_batch<double>(in, out, nsys, std::atoi(argv[5]));
+               ? run_batch<float>(in, out, nsys, std::atoi(argv[5]), forces, every)
+               : run_batch<double>(in, out, nsys, std::atoi(argv[5]), forces, every);
     } catch (const std::exception &e) {
       std::fprintf(stderr, "reference threw: %s\n", e.what());
       rc = 4;
     }
     std::fclose(in);
     std::fclose(out);
+    if (forces) std::fclose(forces);
     return rc;
   }
   if (argc != 5) {

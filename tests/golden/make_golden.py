@@ -15,7 +15,8 @@ nodes.
 
 Output: tests/golden/<case>_<ct>.npz, plus a timing summary on stdout.  The
 case ``batch256`` runs the 256-system uneven batch through the reference one
-system after another and keeps per-system energies and solve times.
+system after another and keeps per-system energies and solve times, and the
+per-atom outputs of every 16th system.
 """
 import json
 import math
@@ -109,8 +110,10 @@ def render_tdesigns(dst):
 
 # The uneven batch: 256 independent water boxes (300-30,000 atoms, two cubature
 # orders, seed 0), run by the reference one system after another (its plain
-# path).  The fixture keeps each system's total energy and solve time.
+# path).  The fixture keeps each system's total energy and solve time, and
+# the per-atom forces and energies of every BATCH_FORCES_EVERY-th system.
 BATCH_CASE = "batch256"
+BATCH_FORCES_EVERY = 16
 
 
 def batch_inputs_sha256(sy):
@@ -129,8 +132,9 @@ def make_batch(work, iters=2):
         with open(lst, "ab") as f, open(rec, "rb") as g:
             f.write(g.read())
     out = os.path.join(work, "batch.out")
-    r = subprocess.run([harness(), "--batch", lst, out, "double", str(iters)], cwd=work, capture_output=True,
-                       text=True)
+    fout = os.path.join(work, "batch.forces")
+    r = subprocess.run([harness(), "--batch", lst, out, "double", str(iters), fout, str(BATCH_FORCES_EVERY)],
+                       cwd=work, capture_output=True, text=True)
     if r.returncode != 0:
         print(r.stdout[-2000:], r.stderr[-2000:])
         raise SystemExit("reference harness failed on the batch (%d)" % r.returncode)
@@ -139,9 +143,23 @@ def make_batch(work, iters=2):
     (nsys,) = struct.unpack_from("<I", data, 0)
     rec = np.dtype([("natom", "<u4"), ("K", "<u4"), ("ms_host", "<f8"), ("ms_events", "<f8"), ("energy", "<f8")])
     o = np.frombuffer(data, dtype=rec, count=nsys, offset=4)
+    # forces of the sampled systems, concatenated in system order
+    with open(fout, "rb") as f:
+        fdata = f.read()
+    idx, parts, off = [], [[], [], [], []], 0
+    while off < len(fdata):
+        s_i, n_i = struct.unpack_from("<II", fdata, off)
+        off += 8
+        idx.append(s_i)
+        for k in range(4):
+            parts[k].append(np.frombuffer(fdata, dtype="<f8", count=n_i, offset=off).copy())
+            off += 8 * n_i
     np.savez_compressed(os.path.join(HERE, BATCH_CASE + "_double.npz"), natom=o["natom"].copy(), K=o["K"].copy(),
                         ms_host=o["ms_host"].copy(), ms_events=o["ms_events"].copy(), energy=o["energy"].copy(),
-                        tol=np.array([s["tol"] for s in sy]), input_sha256=np.array(batch_inputs_sha256(sy)))
+                        tol=np.array([s["tol"] for s in sy]), input_sha256=np.array(batch_inputs_sha256(sy)),
+                        forces_systems=np.array(idx, dtype=np.uint32),
+                        fx=np.concatenate(parts[0]), fy=np.concatenate(parts[1]), fz=np.concatenate(parts[2]),
+                        en=np.concatenate(parts[3]))
     summary = dict(systems=int(nsys), atoms=int(o["natom"].sum()), sequential_ms_host=float(o["ms_host"].sum()),
                    sequential_ms_events=float(o["ms_events"].sum()))
     print(json.dumps({BATCH_CASE + "_double": summary}), flush=True)

@@ -68,7 +68,26 @@ def test_batch256_energies_match_reference(pkg):
     with pkg.GlstBatch(sy, nstreams=16) as b:
         b.compute(*ins, *outs)
         e = b.energies()
+        off = b.offsets
+        got = [o.cpu().numpy() for o in outs]
     ref = gold["energy"]
     assert np.array_equal(gold["natom"], [s["natom"] for s in sy])
     rel = np.abs(e - ref) / np.abs(ref)
     assert rel.max() <= 1e-7, (int(rel.argmax()), float(rel.max()))
+    # per-atom forces and energies of every 16th system against the
+    # reference's own outputs: <= 1e-5 relative force RMS per system
+    if "forces_systems" not in gold:
+        pytest.skip("batch256 fixture has no per-atom outputs")
+    from oracle import oracle
+    at = 0
+    worst = 0.0
+    for i in gold["forces_systems"]:
+        n_i = int(gold["natom"][i])
+        ref_i = [gold[k][at:at + n_i] for k in ("fx", "fy", "fz", "en")]
+        got_i = [a[off[i]:off[i + 1]] for a in got]
+        rep = oracle.error_report(got_i, ref_i)
+        assert rep["force_rms_rel"] <= 1e-5 and rep["energy_rel"] <= 1e-7, (int(i), rep)
+        worst = max(worst, rep["force_rms_rel"])
+        at += n_i
+    assert at == len(gold["fx"])
+    print("batch256: %d systems' forces, worst relative force RMS %.3g" % (len(gold["forces_systems"]), worst))

@@ -293,6 +293,49 @@ def test_node_shards_sum_to_the_full_result(pkg, nshards):
     assert abs(e_sum - e_full) <= 1e-12 * abs(e_full)
 
 
+class _DeviceArray:
+    """A device pointer of n doubles, readable by torch (CUDA array interface)."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 2}
+
+
+def _cell_outputs(f, n):
+    """The cell-ordered outputs (the reference's fx()..en()), copied to host."""
+    return [torch.as_tensor(_DeviceArray(p, n), device="cuda:0").cpu().numpy().copy() for p in f.cell_outputs()]
+
+
+@pytest.mark.parametrize("nshards", [2, 4])
+def test_reduce_shards_in_library(pkg, nshards):
+    """glst_reduce_shards (the reference's reduce of the shards' outputs to
+    the first GPU): shards computed on their own streams, summed by shard 0's
+    device in shard order -- here all on one device, so the peer reads are
+    local; the result in shard 0 equals the unsharded solve, input order, cell
+    order and total energy."""
+    n_mol, L, rcut, tol, seed = SYSTEMS["w2000_tol1e-5"]
+    x, y, z, q = _water(n_mol, L, seed)
+    d = [_dev(a) for a in (x, y, z, q)]
+    f, full = _run(pkg, x, y, z, q, tol, L, rcut)
+    e_full = f.energy()
+    cell_full = _cell_outputs(f, len(x))
+    f.close()
+    streams = [torch.cuda.Stream() for _ in range(nshards)]
+    shards = [pkg.GlstForce(len(x), tol, L, L, L, rcut=rcut, shard=(s, nshards)) for s in range(nshards)]
+    torch.cuda.synchronize()  # inputs in place before the shards' streams read them
+    for sh, st in zip(shards, streams):
+        sh.calc_ener_force(*d, stream=st)
+    pkg.reduce_shards(shards, streams)
+    got = shards[0].get_ef(stream=streams[0])
+    rep = oracle.error_report(got, full)
+    assert rep["force_rms_rel"] < 1e-12 and rep["energy_rel"] < 1e-12, rep
+    assert abs(shards[0].energy(stream=streams[0]) - e_full) <= 1e-12 * abs(e_full)
+    torch.cuda.synchronize()
+    cell = _cell_outputs(shards[0], len(x))
+    assert oracle.error_report(cell, cell_full)["force_rms_rel"] < 1e-12
+    for sh in shards:
+        sh.close()
+
+
 def test_autotune_keeps_results(pkg, store):
     """glst_autotune changes launch shapes only: the tuned handle, and a new
     handle of the same shape that inherits the tuning, stay within the parity
