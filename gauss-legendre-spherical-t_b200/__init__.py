@@ -358,7 +358,10 @@ class GlstBatch:
     systems: sequence of dicts with natom, tol, box (3), rcut.  Inputs and
     outputs are concatenated in system order (``offsets`` gives the starts).
     ``compute(..., plain=False)`` runs one captured CUDA graph over all
-    systems; ``plain=True`` solves them one after another (baseline).
+    systems (one persistent launch per phase over a work list of every
+    system's blocks, beside the launch sequences of systems that do not fit
+    the work-list kernels); ``plain=True`` solves them one after another
+    (baseline).
     """
 
     def __init__(self, systems, ct="double", nstreams=16):
@@ -393,9 +396,16 @@ class GlstBatch:
     def __exit__(self, *exc):
         self.close()
 
-    def compute(self, x, y, z, q, fx, fy, fz, en, plain=False, stream=None):
+    MODES = {"worklist": 0, "plain": 1, "branches": 2}
+
+    def compute(self, x, y, z, q, fx, fy, fz, en, plain=False, stream=None, mode=None):
+        """mode: "worklist" (default; one launch per phase for every system
+        that fits the work-list kernels, the others on graph branches),
+        "branches" (every system its own launch sequence, graph branches),
+        "plain" (one system after another; also plain=True)."""
+        m = self.MODES[mode] if mode is not None else (1 if plain else 0)
         _check(self._lib.glst_batch_compute(self._b, _ptr(x), _ptr(y), _ptr(z), _ptr(q), _ptr(fx), _ptr(fy),
-                                            _ptr(fz), _ptr(en), 1 if plain else 0, _stream(stream)))
+                                            _ptr(fz), _ptr(en), m, _stream(stream)))
 
     def energies(self, stream=None):
         e = np.empty(self.nsys)

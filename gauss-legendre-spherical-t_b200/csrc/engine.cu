@@ -18,7 +18,7 @@
 #include <cuda_runtime.h>
 
 #include "glst_c.h"
-#include "kernels.cuh"
+#include "worklist.cuh"
 #include "planner.hpp"
 
 using glst::Plan;
@@ -1415,7 +1415,19 @@ struct glst_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   const void *key[8] = {};
+  int key_mode = -1;                    // mode the graph was captured in
   double *energies = nullptr;           // device, one per system
+  // Work list: systems solved by one persistent launch per phase (the rest
+  // keep their own launch sequences on the other branches).
+  std::vector<uint32_t> wl;             // batch indices of the work-list systems
+  std::vector<uint8_t> in_wl;           // per system
+  enum { kZero, kBin, kScan, kScatter, kSort, kSf, kShell, kLr, kSr, kCombine, kEnergy, kPhases };
+  uint32_t ph_off[kPhases] = {}, ph_n[kPhases] = {}, ph_grid[kPhases] = {};
+  dev::WorkItem *d_items = nullptr;
+  dev::SysDesc *d_desc = nullptr;
+  size_t shell_smem = 0;                // dynamic shared memory of the shell-sum launch
+  cudaStream_t wl_side = nullptr;       // near field of the work list, beside its far field
+  cudaEvent_t wl_fork = nullptr, wl_join = nullptr;
 };
 
 static constexpr uint32_t kBatchLargeAtoms = 20000;  // fills the GPU by itself
@@ -1441,9 +1453,201 @@ static void batch_release(glst_batch *b) {
   if (b->ev_in) cudaEventDestroy(b->ev_in);
   if (b->ev_out) cudaEventDestroy(b->ev_out);
   if (b->energies) cudaFree(b->energies);
+  if (b->d_items) cudaFree(b->d_items);
+  if (b->d_desc) cudaFree(b->d_desc);
+  if (b->wl_side) cudaStreamDestroy(b->wl_side);
+  if (b->wl_fork) cudaEventDestroy(b->wl_fork);
+  if (b->wl_join) cudaEventDestroy(b->wl_join);
   b->own = nullptr;
   b->ev_in = b->ev_out = nullptr;
   b->energies = nullptr;
+  b->d_items = nullptr;
+  b->d_desc = nullptr;
+  b->wl_side = nullptr;
+  b->wl_fork = b->wl_join = nullptr;
+}
+
+// A system joins the work list when its solve is one launch of each kernel
+// with the shapes the work-list kernels use: whole system, one node stage,
+// shell sums in shared memory with several nodes per CTA (or no far field).
+static bool worklist_ok(const glst_handle *h) {
+  if (h->nshards != 1 || h->ranges.size() > 1 || h->gsat) return false;
+  if (h->K && h->sat_nb < 2) return false;
+  if ((h->plan.ncell + dev::kSfCellsPerCta - 1) / dev::kSfCellsPerCta > 65535u) return false;
+  return true;
+}
+
+// Work items of every phase for the work-list systems, and the persistent
+// grid of each phase's kernel (resident CTAs on every SM, at most one per item).
+static glst_status worklist_build(glst_batch *b) {
+  b->wl.clear();
+  b->in_wl.assign(b->sys.size(), 0);
+  for (uint32_t i = 0; i < b->sys.size(); i++)
+    if (worklist_ok(b->sys[i])) {
+      b->wl.push_back(i);
+      b->in_wl[i] = 1;
+    }
+  if (b->wl.empty()) return GLST_OK;
+  std::vector<dev::WorkItem> items;
+  auto begin = [&](int ph) { b->ph_off[ph] = (uint32_t)items.size(); };
+  auto end = [&](int ph) { b->ph_n[ph] = (uint32_t)items.size() - b->ph_off[ph]; };
+  const uint32_t nw = (uint32_t)b->wl.size();
+  auto each = [&](int ph, auto &&fn) {
+    begin(ph);
+    for (uint32_t w = 0; w < nw; w++) fn(w, b->sys[b->wl[w]]);
+    end(ph);
+  };
+  each(glst_batch::kZero, [&](uint32_t w, glst_handle *h) {
+    for (uint32_t c = 0; c < (h->plan.ncell + 1023) / 1024; c++) items.push_back({w, c, 0, 0});
+  });
+  each(glst_batch::kBin, [&](uint32_t w, glst_handle *h) {
+    for (uint32_t a = 0; a < (h->plan.natom + 255) / 256; a++) items.push_back({w, a, 0, 0});
+  });
+  each(glst_batch::kScan, [&](uint32_t w, glst_handle *) { items.push_back({w, 0, 0, 0}); });
+  each(glst_batch::kScatter, [&](uint32_t w, glst_handle *h) {
+    for (uint32_t a = 0; a < (h->plan.natom + 255) / 256; a++) items.push_back({w, a, 0, 0});
+  });
+  each(glst_batch::kSort, [&](uint32_t w, glst_handle *h) {
+    if (h->plan.natom)
+      for (uint32_t c = 0; c < h->plan.ncell; c++) items.push_back({w, c, 0, 0});
+  });
+  each(glst_batch::kSf, [&](uint32_t w, glst_handle *h) {
+    if (!h->K || !h->plan.natom) return;
+    const uint32_t rows = (h->plan.ncell + dev::kSfCellsPerCta - 1) / dev::kSfCellsPerCta;
+    for (uint32_t r = 0; r < rows; r++)
+      for (uint32_t u = 0; u < h->n_sf_units; u++) items.push_back({w, u, r, 0});
+  });
+  each(glst_batch::kShell, [&](uint32_t w, glst_handle *h) {
+    if (!h->K || !h->plan.natom) return;
+    for (uint32_t k = 0; k < (h->K + h->sat_nb - 1) / h->sat_nb; k++) items.push_back({w, k, 0, 0});
+  });
+  each(glst_batch::kLr, [&](uint32_t w, glst_handle *h) {
+    if (!h->K || !h->plan.natom) return;
+    const uint32_t ab = (h->plan.natom + dev::kLrThreads - 1) / dev::kLrThreads;
+    for (uint32_t c = 0; c < h->nsplit; c++)
+      for (uint32_t a = 0; a < ab; a++) items.push_back({w, a, c, 0});
+  });
+  each(glst_batch::kSr, [&](uint32_t w, glst_handle *h) {
+    if (!h->plan.natom) return;
+    for (uint32_t pl = 0; pl < (uint32_t)dev::kSrPlanes; pl++)
+      for (uint32_t c = 0; c < h->plan.ncell; c++) items.push_back({w, c, pl, 0});
+  });
+  each(glst_batch::kCombine, [&](uint32_t w, glst_handle *h) {
+    if (h->plan.natom)
+      for (uint32_t a = 0; a < h->combine_blocks; a++) items.push_back({w, a, 0, 0});
+  });
+  each(glst_batch::kEnergy, [&](uint32_t w, glst_handle *) { items.push_back({w, 0, 0, 0}); });
+  CUDA_TRY(cudaMalloc(&b->d_items, std::max<size_t>(1, items.size()) * sizeof(dev::WorkItem)));
+  CUDA_TRY(cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(dev::WorkItem), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMalloc(&b->d_desc, nw * sizeof(dev::SysDesc)));
+  // shell sums: the largest work-list system's shared memory
+  b->shell_smem = 0;
+  for (uint32_t i : b->wl) {
+    const glst_handle *h = b->sys[i];
+    if (!h->K) continue;
+    const bool table = h->sat_xyz && h->sat_nb > 1;
+    b->shell_smem = std::max(b->shell_smem, h->sat_per_node * h->sat_nb +
+                                                (table ? (((size_t)h->plan.ncell * 4 + 15) & ~size_t(15)) : 0));
+  }
+  int nsm = 148, smem_optin = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device));
+  CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device));
+  CUDA_TRY(cudaFuncSetAttribute(dev::k_shell_sums_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin));
+  CUDA_TRY(cudaFuncSetAttribute(dev::k_sort_pack_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(dev::kSortCap * sizeof(uint32_t))));
+  auto grid = [&](int ph, const void *fn, int threads, size_t smem) -> glst_status {
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+    b->ph_grid[ph] = std::max<uint32_t>(1, std::min<uint32_t>(b->ph_n[ph], (uint32_t)std::max(1, per_sm) * nsm));
+    return GLST_OK;
+  };
+  GLST_TRY(grid(glst_batch::kZero, (const void *)dev::k_zero_counts_multi, 1024, 0));
+  GLST_TRY(grid(glst_batch::kBin, (const void *)dev::k_bin_multi, 256, 0));
+  GLST_TRY(grid(glst_batch::kScan, (const void *)dev::k_scan_multi, 1024, 0));
+  GLST_TRY(grid(glst_batch::kScatter, (const void *)dev::k_scatter_multi, 256, 0));
+  GLST_TRY(grid(glst_batch::kSort, (const void *)dev::k_sort_pack_multi, 256, dev::kSortCap * sizeof(uint32_t)));
+  GLST_TRY(grid(glst_batch::kSf, (const void *)dev::k_structure_factors_multi, dev::kSfThreads, 0));
+  GLST_TRY(grid(glst_batch::kShell, (const void *)dev::k_shell_sums_multi, dev::kSatThreads, b->shell_smem));
+  GLST_TRY(grid(glst_batch::kLr, (const void *)dev::k_long_range_multi, dev::kLrThreads, 0));
+  GLST_TRY(grid(glst_batch::kSr, (const void *)dev::k_short_range_multi, dev::kSrThreads, 0));
+  GLST_TRY(grid(glst_batch::kCombine, (const void *)dev::k_combine_multi, dev::kCombineThreads, 0));
+  GLST_TRY(grid(glst_batch::kEnergy, (const void *)dev::k_energy_multi, 256, 0));
+  CUDA_TRY(cudaStreamCreateWithFlags(&b->wl_side, cudaStreamNonBlocking));
+  CUDA_TRY(cudaEventCreateWithFlags(&b->wl_fork, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&b->wl_join, cudaEventDisableTiming));
+  return GLST_OK;
+}
+
+// Descriptors of the work-list systems for these inputs and outputs
+// (uploaded before the graph is captured; the graph reads them).
+static glst_status worklist_descriptors(glst_batch *b, const double *const in[4], double *const out[4]) {
+  std::vector<dev::SysDesc> ds(b->wl.size());
+  for (size_t w = 0; w < b->wl.size(); w++) {
+    const uint32_t i = b->wl[w];
+    const glst_handle *h = b->sys[i];
+    const size_t o = b->off[i];
+    dev::SysDesc &d = ds[w];
+    std::memset(&d, 0, sizeof d);
+    d.g = h->grid;
+    d.natom = h->plan.natom;
+    d.combine_blocks = h->combine_blocks;
+    d.part_rows = h->part_rows;
+    d.use_far = h->K ? 1u : 0u;
+    if (h->K) {
+      uint32_t lg = 0;
+      while ((1u << lg) < h->sat_nb) lg++;
+      const bool table = h->sat_xyz && h->sat_nb > 1;
+      d.sat = dev::SatArgs{h->S, h->node64, h->node_radii, h->K, 0, h->sat_nb, lg, table ? 1u : 0u,
+                           h->sat_stride, h->R};
+    }
+    d.rx = in[0] + o; d.ry = in[1] + o; d.rz = in[2] + o; d.qc = in[3] + o;
+    d.atom_cell = h->atom_cell; d.atom_slot = h->atom_slot; d.perm = h->perm;
+    d.sorted_idx = h->sorted_idx; d.cell_count = h->cell_count; d.cell_point = h->cell_point;
+    d.pk = h->pk; d.pd = h->pd; d.dirs = h->dirs; d.kappa = h->kappa;
+    d.chunks = h->chunks; d.sf_units = h->sf_units;
+    d.S = h->S; d.R = h->R; d.part = h->part; d.sr = h->sr;
+    d.cfx = h->cfx; d.cfy = h->cfy; d.cfz = h->cfz; d.cen = h->cen;
+    // input-order outputs straight into the batch's arrays (or the
+    // handle's own when the caller passes none)
+    d.ofx = out[0] ? out[0] + o : h->ofx;
+    d.ofy = out[1] ? out[1] + o : h->ofy;
+    d.ofz = out[2] ? out[2] + o : h->ofz;
+    d.oen = out[3] ? out[3] + o : h->oen;
+    d.block_energy = h->block_energy;
+    d.energy = b->energies + i;
+  }
+  if (!ds.empty()) CUDA_TRY(cudaMemcpy(b->d_desc, ds.data(), ds.size() * sizeof(dev::SysDesc), cudaMemcpyHostToDevice));
+  return GLST_OK;
+}
+
+// The work-list solve on stream st: one launch per phase for all its systems;
+// the near field on a side stream beside the far field.
+static glst_status worklist_launch(glst_batch *b, cudaStream_t st) {
+  const dev::SysDesc *D = b->d_desc;
+  auto it = [&](int ph) { return b->d_items + b->ph_off[ph]; };
+  auto go = [&](int ph, auto kern, int threads, size_t smem, cudaStream_t s) -> glst_status {
+    if (!b->ph_n[ph]) return GLST_OK;
+    kern<<<b->ph_grid[ph], threads, smem, s>>>(D, it(ph), b->ph_n[ph]);
+    CUDA_TRY(cudaGetLastError());
+    return GLST_OK;
+  };
+  GLST_TRY(go(glst_batch::kZero, dev::k_zero_counts_multi, 1024, 0, st));
+  GLST_TRY(go(glst_batch::kBin, dev::k_bin_multi, 256, 0, st));
+  GLST_TRY(go(glst_batch::kScan, dev::k_scan_multi, 1024, 0, st));
+  GLST_TRY(go(glst_batch::kScatter, dev::k_scatter_multi, 256, 0, st));
+  GLST_TRY(go(glst_batch::kSort, dev::k_sort_pack_multi, 256, dev::kSortCap * sizeof(uint32_t), st));
+  GLST_TRY(go(glst_batch::kSf, dev::k_structure_factors_multi, dev::kSfThreads, 0, st));
+  // near field forked after the structure factors, as in a single solve
+  CUDA_TRY(cudaEventRecord(b->wl_fork, st));
+  CUDA_TRY(cudaStreamWaitEvent(b->wl_side, b->wl_fork, 0));
+  GLST_TRY(go(glst_batch::kSr, dev::k_short_range_multi, dev::kSrThreads, 0, b->wl_side));
+  CUDA_TRY(cudaEventRecord(b->wl_join, b->wl_side));
+  GLST_TRY(go(glst_batch::kShell, dev::k_shell_sums_multi, dev::kSatThreads, b->shell_smem, st));
+  GLST_TRY(go(glst_batch::kLr, dev::k_long_range_multi, dev::kLrThreads, 0, st));
+  CUDA_TRY(cudaStreamWaitEvent(st, b->wl_join, 0));
+  GLST_TRY(go(glst_batch::kCombine, dev::k_combine_multi, dev::kCombineThreads, 0, st));
+  GLST_TRY(go(glst_batch::kEnergy, dev::k_energy_multi, 256, 0, st));
+  return GLST_OK;
 }
 
 // One system: solve, then copy its outputs into the batch's arrays.
@@ -1459,18 +1663,30 @@ static glst_status batch_one(glst_batch *b, uint32_t i, const double *const in[4
   return GLST_OK;
 }
 
-static glst_status batch_capture(glst_batch *b, const double *const in[4], double *const out[4]) {
+// Graph of one batched solve.  mode 0: the work-list systems by one launch
+// per phase on branch 0, every other system its own launch sequence on the
+// remaining branches; mode 2: every system its own launch sequence on the
+// branches (large systems on branch 0, the rest spread over the others).
+static glst_status batch_capture(glst_batch *b, const double *const in[4], double *const out[4], int mode) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   b->exec = nullptr;
   b->graph = nullptr;
+  const bool wl = mode == 0 && !b->wl.empty();
+  if (wl) GLST_TRY(worklist_descriptors(b, in, out));
   CUDA_TRY(cudaStreamBeginCapture(b->own, cudaStreamCaptureModeThreadLocal));
   glst_status s = GLST_OK;
   cudaError_t e = cudaEventRecord(b->ev_in, b->own);
   for (size_t j = 0; e == cudaSuccess && j < b->branch.size(); j++) e = cudaStreamWaitEvent(b->branch[j], b->ev_in, 0);
+  if (e == cudaSuccess && wl) s = worklist_launch(b, b->branch[0]);
+  const size_t nbr = b->branch.size();
+  size_t next = 0;  // round robin over branches 1.. for the others in work-list mode
   for (size_t t = 0; e == cudaSuccess && s == GLST_OK && t < b->order.size(); t++) {
     const uint32_t i = b->order[t];
-    s = batch_one(b, i, in, out, b->branch[b->branch_of[i]]);
+    if (wl && b->in_wl[i]) continue;
+    cudaStream_t st = b->branch[b->branch_of[i]];
+    if (wl) st = b->branch[nbr > 1 ? 1 + (next++ % (nbr - 1)) : 0];
+    s = batch_one(b, i, in, out, st);
   }
   for (size_t j = 0; e == cudaSuccess && j < b->branch.size(); j++) {
     e = cudaEventRecord(b->branch_done[j], b->branch[j]);
@@ -1493,6 +1709,7 @@ static glst_status batch_capture(glst_batch *b, const double *const in[4], doubl
     b->key[k] = in[k];
     b->key[4 + k] = out[k];
   }
+  b->key_mode = mode;
   return GLST_OK;
 }
 
@@ -1555,6 +1772,13 @@ glst_status glst_batch_create(glst_batch **out, uint32_t nsys, const uint32_t *n
   CUDA_TRY(cudaEventCreateWithFlags(&b->ev_out, cudaEventDisableTiming));
   CUDA_TRY(cudaMalloc(&b->energies, sizeof(double) * std::max<uint32_t>(1, nsys)));
   CUDA_TRY(cudaMemset(b->energies, 0, sizeof(double) * std::max<uint32_t>(1, nsys)));
+  {
+    const glst_status ws = worklist_build(b.get());
+    if (ws != GLST_OK) {
+      batch_release(b.get());
+      return ws;
+    }
+  }
   *out = b.release();
   return GLST_OK;
 }
@@ -1588,13 +1812,14 @@ glst_status glst_batch_compute(glst_batch *b, const double *rx, const double *ry
   const double *in[4] = {rx, ry, rz, qc};
   double *out[4] = {fx, fy, fz, en};
   cudaStream_t st = S_(stream);
-  if (plain) {
+  if (plain == 1) {
     for (uint32_t i = 0; i < b->sys.size(); i++) GLST_TRY(batch_one(b, i, in, out, st));
     return GLST_OK;
   }
-  bool same = b->exec != nullptr;
+  if (plain != 0 && plain != 2) return fail(GLST_ERR_INVALID_ARG, "mode must be 0, 1 or 2");
+  bool same = b->exec != nullptr && b->key_mode == plain;
   for (int k = 0; k < 4 && same; k++) same = b->key[k] == in[k] && b->key[4 + k] == out[k];
-  if (!same) GLST_TRY(batch_capture(b, in, out));
+  if (!same) GLST_TRY(batch_capture(b, in, out, plain));
   CUDA_TRY(cudaEventRecord(b->ev_in, st));
   CUDA_TRY(cudaStreamWaitEvent(b->own, b->ev_in, 0));
   CUDA_TRY(cudaGraphLaunch(b->exec, b->own));

@@ -70,11 +70,13 @@ __device__ __forceinline__ uint32_t bin_axis(double r, const Grid &g, uint32_t n
 }
 
 // K_bin: cell of every atom and an (unordered) slot inside the cell.
-__global__ void k_bin(const double *__restrict__ rx, const double *__restrict__ ry,
-                      const double *__restrict__ rz, uint32_t n, Grid g,
-                      uint32_t *__restrict__ atom_cell, uint32_t *__restrict__ atom_slot,
-                      uint32_t *__restrict__ cell_count) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+// (Each kernel's body is a device function of its block indices, so that
+// the batched work-list kernels can run the same code for many systems.)
+__device__ __forceinline__ void bin_block(const double *__restrict__ rx, const double *__restrict__ ry,
+                                          const double *__restrict__ rz, uint32_t n, const Grid &g,
+                                          uint32_t *__restrict__ atom_cell, uint32_t *__restrict__ atom_slot,
+                                          uint32_t *__restrict__ cell_count, uint32_t bx) {
+  const uint32_t i = bx * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t cx = bin_axis(rx[i], g, g.nx);
   const uint32_t cy = bin_axis(ry[i], g, g.ny);
@@ -84,10 +86,17 @@ __global__ void k_bin(const double *__restrict__ rx, const double *__restrict__ 
   atom_slot[i] = atomicAdd(&cell_count[cell], 1u);
 }
 
+__global__ void k_bin(const double *__restrict__ rx, const double *__restrict__ ry,
+                      const double *__restrict__ rz, uint32_t n, Grid g,
+                      uint32_t *__restrict__ atom_cell, uint32_t *__restrict__ atom_slot,
+                      uint32_t *__restrict__ cell_count) {
+  bin_block(rx, ry, rz, n, g, atom_cell, atom_slot, cell_count, blockIdx.x);
+}
+
 // K_scan: exclusive offsets of the cell counts (one CTA of 1024 threads,
 // chunked block scan).
-__global__ void k_scan(const uint32_t *__restrict__ cell_count, uint32_t ncell,
-                       uint32_t *__restrict__ cell_point) {
+__device__ __forceinline__ void scan_body(const uint32_t *__restrict__ cell_count, uint32_t ncell,
+                                          uint32_t *__restrict__ cell_point) {
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t carry;
   if (threadIdx.x == 0) carry = 0;
@@ -123,13 +132,25 @@ __global__ void k_scan(const uint32_t *__restrict__ cell_count, uint32_t ncell,
   }
 }
 
+__global__ void k_scan(const uint32_t *__restrict__ cell_count, uint32_t ncell,
+                       uint32_t *__restrict__ cell_point) {
+  scan_body(cell_count, ncell, cell_point);
+}
+
+__device__ __forceinline__ void scatter_block(const uint32_t *__restrict__ atom_cell,
+                                              const uint32_t *__restrict__ atom_slot,
+                                              const uint32_t *__restrict__ cell_point, uint32_t n,
+                                              uint32_t *__restrict__ perm, uint32_t bx) {
+  const uint32_t i = bx * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  perm[cell_point[atom_cell[i]] + atom_slot[i]] = i;
+}
+
 __global__ void k_scatter(const uint32_t *__restrict__ atom_cell,
                           const uint32_t *__restrict__ atom_slot,
                           const uint32_t *__restrict__ cell_point, uint32_t n,
                           uint32_t *__restrict__ perm) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  perm[cell_point[atom_cell[i]] + atom_slot[i]] = i;
+  scatter_block(atom_cell, atom_slot, cell_point, n, perm, blockIdx.x);
 }
 
 // K_sort_pack: one CTA per cell.  The atomics of k_bin leave the atoms of a
@@ -149,16 +170,15 @@ __device__ __forceinline__ void pack_atom(uint32_t slot, uint32_t a, double cx, 
                          static_cast<float>(q));
 }
 
-__global__ void k_sort_pack(const uint32_t *__restrict__ perm,
-                            const uint32_t *__restrict__ cell_count,
-                            const uint32_t *__restrict__ cell_point, Grid g,
-                            const uint32_t *__restrict__ atom_cell, uint32_t natom,
-                            const double *__restrict__ rx, const double *__restrict__ ry,
-                            const double *__restrict__ rz, const double *__restrict__ qc,
-                            uint32_t *__restrict__ sorted_idx, float4 *__restrict__ pk,
-                            double4 *__restrict__ pd) {
+__device__ __forceinline__ void sort_pack_block(const uint32_t *__restrict__ perm,
+                                                const uint32_t *__restrict__ cell_count,
+                                                const uint32_t *__restrict__ cell_point, const Grid &g,
+                                                const uint32_t *__restrict__ atom_cell, uint32_t natom,
+                                                const double *__restrict__ rx, const double *__restrict__ ry,
+                                                const double *__restrict__ rz, const double *__restrict__ qc,
+                                                uint32_t *__restrict__ sorted_idx, float4 *__restrict__ pk,
+                                                double4 *__restrict__ pd, uint32_t cell) {
   extern __shared__ uint32_t s_idx[];
-  const uint32_t cell = blockIdx.x;
   const uint32_t cnt = cell_count[cell];
   const uint32_t start = cell_point[cell];
   if (cnt == 0) return;
@@ -216,6 +236,18 @@ __global__ void k_sort_pack(const uint32_t *__restrict__ perm,
   }
   for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
     pack_atom(start + i, s_idx[i], cx, cy, cz, rx, ry, rz, qc, sorted_idx, pk, pd);
+}
+
+__global__ void k_sort_pack(const uint32_t *__restrict__ perm,
+                            const uint32_t *__restrict__ cell_count,
+                            const uint32_t *__restrict__ cell_point, Grid g,
+                            const uint32_t *__restrict__ atom_cell, uint32_t natom,
+                            const double *__restrict__ rx, const double *__restrict__ ry,
+                            const double *__restrict__ rz, const double *__restrict__ qc,
+                            uint32_t *__restrict__ sorted_idx, float4 *__restrict__ pk,
+                            double4 *__restrict__ pd) {
+  sort_pack_block(perm, cell_count, cell_point, g, atom_cell, natom, rx, ry, rz, qc, sorted_idx, pk, pd,
+                  blockIdx.x);
 }
 
 // ----------------------------------------------------------------------------
@@ -447,15 +479,16 @@ __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restric
 // node_off on (a node range of the handle: the whole of it, or one stage).
 // Cells: kSfCellsPerCta per CTA row from cell_base on (grids of more than
 // 65,535 rows take several launches).  lo_buf: scratch of S's size.
-__global__ void __launch_bounds__(kSfThreads, 8)
-k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_count,
-                    const uint32_t *__restrict__ cell_point, Grid g, const SfUnit *__restrict__ units,
-                    const float4 *__restrict__ dirs, const float *__restrict__ kappa, uint32_t node_off,
-                    uint32_t cell_base, float2 *__restrict__ S, float2 *__restrict__ lo_buf) {
+__device__ __forceinline__ void sf_block(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_count,
+                                         const uint32_t *__restrict__ cell_point, const Grid &g,
+                                         const SfUnit *__restrict__ units, const float4 *__restrict__ dirs,
+                                         const float *__restrict__ kappa, uint32_t node_off, uint32_t cell_base,
+                                         float2 *__restrict__ S, float2 *__restrict__ lo_buf, uint32_t bx,
+                                         uint32_t by) {
   __shared__ float4 s_at[kSfAtomTile];
   __shared__ float2 s_f[kSfThreads * kSfMaxNpt];
-  const SfUnit u = units[blockIdx.x];
-  const uint32_t c0 = cell_base + blockIdx.y * kSfCellsPerCta;
+  const SfUnit u = units[bx];
+  const uint32_t c0 = cell_base + by * kSfCellsPerCta;
   const uint32_t c1 = min(g.ncell, c0 + kSfCellsPerCta);
 #define GLST_SF_CASE(n) \
   case n: sf_unit<n>(u, pk, cell_count, cell_point, g, dirs, kappa, c0, c1, node_off, S, lo_buf, s_at, s_f); break;
@@ -465,6 +498,15 @@ k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ 
     default: break;
   }
 #undef GLST_SF_CASE
+}
+
+__global__ void __launch_bounds__(kSfThreads, 8)
+k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_count,
+                    const uint32_t *__restrict__ cell_point, Grid g, const SfUnit *__restrict__ units,
+                    const float4 *__restrict__ dirs, const float *__restrict__ kappa, uint32_t node_off,
+                    uint32_t cell_base, float2 *__restrict__ S, float2 *__restrict__ lo_buf) {
+  sf_block(pk, cell_count, cell_point, g, units, dirs, kappa, node_off, cell_base, S, lo_buf, blockIdx.x,
+           blockIdx.y);
 }
 
 // ----------------------------------------------------------------------------
@@ -534,12 +576,11 @@ __device__ __forceinline__ double2 box_padded(const double2 *row, uint32_t xl, u
 // lines the warp takes per step, so the per-node values (radii, weight,
 // twiddle rows) stay in registers and the S loads and R stores of a warp are
 // runs of consecutive nodes.
-template <int kThreads, int kMinBlocks>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
-k_shell_sums(Grid g, SatArgs a) {
+template <int kMinBlocks>
+__device__ __forceinline__ void shell_block(const Grid &g, const SatArgs &a, uint32_t bx) {
   extern __shared__ double2 s_sat[];
   const uint32_t nb = a.nb, lg = a.lg_nb;
-  const uint32_t k0 = blockIdx.x * nb;
+  const uint32_t k0 = bx * nb;
   const uint32_t C = g.ncell;
   const uint32_t naxis = g.nx + g.ny + g.nz;
   const uint32_t sy = g.nz + 1, sx = (g.ny + 1) * sy;  // padded strides
@@ -699,6 +740,12 @@ k_shell_sums(Grid g, SatArgs a) {
       x += dx;
     }
   }
+}
+
+template <int kThreads, int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+k_shell_sums(Grid g, SatArgs a) {
+  shell_block<kMinBlocks>(g, a, blockIdx.x);
 }
 
 // ----------------------------------------------------------------------------
@@ -913,18 +960,18 @@ __device__ __forceinline__ uint32_t cell_of_atom(const uint32_t *__restrict__ ce
   return lo;
 }
 
-__global__ void __launch_bounds__(kLrThreads, 8)
-k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_point, uint32_t ncell,
-                  const LrChunk *__restrict__ chunks, const float4 *__restrict__ dirs,
-                  const float *__restrict__ kappa, const float2 *__restrict__ R, uint32_t node_off,
-                  uint32_t natom, int accumulate, double4 *__restrict__ part) {
+__device__ __forceinline__ void lr_block(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_point,
+                                         uint32_t ncell, const LrChunk *__restrict__ chunks,
+                                         const float4 *__restrict__ dirs, const float *__restrict__ kappa,
+                                         const float2 *__restrict__ R, uint32_t node_off, uint32_t natom,
+                                         int accumulate, double4 *__restrict__ part, uint32_t bx, uint32_t by) {
   __shared__ float4 s_n[2][kLrfCells * kLrfSlot];
   __shared__ float4 s_kappa4[kLrfTilePairs / 2];
   __shared__ uint32_t s_range[2];
-  const uint32_t a0 = blockIdx.x * kLrThreads;
+  const uint32_t a0 = bx * kLrThreads;
   const uint32_t p = a0 + threadIdx.x;
   const bool active = p < natom;
-  const LrChunk ch = chunks[blockIdx.y];
+  const LrChunk ch = chunks[by];
   const uint32_t nr = ch.n_rad;
   const uint32_t npr = (nr + 1) >> 1;                                   // pairs per direction
   const uint32_t dirs_per_tile = max(1u, (uint32_t)kLrfTilePairs / npr);  // npr <= kLrfTilePairs (host check)
@@ -1056,7 +1103,7 @@ k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ ce
   }
   if (active) {
     const double q = static_cast<double>(pa.w);
-    double4 *dst = part + (size_t)blockIdx.y * natom + p;
+    double4 *dst = part + (size_t)by * natom + p;
     double4 v = make_double4(q * ex, q * ey, q * ez, q * ee);
     if (accumulate) {  // a later node stage adds into the same rows
       const double4 o = *dst;
@@ -1064,6 +1111,15 @@ k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ ce
     }
     *dst = v;
   }
+}
+
+__global__ void __launch_bounds__(kLrThreads, 8)
+k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_point, uint32_t ncell,
+                  const LrChunk *__restrict__ chunks, const float4 *__restrict__ dirs,
+                  const float *__restrict__ kappa, const float2 *__restrict__ R, uint32_t node_off,
+                  uint32_t natom, int accumulate, double4 *__restrict__ part) {
+  lr_block(pk, cell_point, ncell, chunks, dirs, kappa, R, node_off, natom, accumulate, part, blockIdx.x,
+           blockIdx.y);
 }
 
 // ----------------------------------------------------------------------------
@@ -1077,13 +1133,11 @@ k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ ce
 constexpr int kSrThreads = 128;
 constexpr int kSrPlanes = 3;
 
-__global__ void __launch_bounds__(kSrThreads)
-k_short_range(const double4 *__restrict__ pd, const uint32_t *__restrict__ cell_count,
-              const uint32_t *__restrict__ cell_point, Grid g, uint32_t natom,
-              double4 *__restrict__ sr) {
+__device__ __forceinline__ void sr_block(const double4 *__restrict__ pd, const uint32_t *__restrict__ cell_count,
+                                         const uint32_t *__restrict__ cell_point, const Grid &g, uint32_t natom,
+                                         double4 *__restrict__ sr, uint32_t cell, uint32_t by) {
   __shared__ double4 s_at[kSrThreads];
-  const uint32_t cell = blockIdx.x;
-  const int plane = static_cast<int>(blockIdx.y) - 1;  // dx of the neighbour plane
+  const int plane = static_cast<int>(by) - 1;  // dx of the neighbour plane
   const uint32_t cnt = cell_count[cell];
   const uint32_t start = cell_point[cell];
   const int ix = cell / (g.ny * g.nz), iy = (cell / g.nz) % g.ny, iz = cell % g.nz;
@@ -1125,8 +1179,15 @@ k_short_range(const double4 *__restrict__ pd, const uint32_t *__restrict__ cell_
         }
       }
     }
-    if (active) sr[(size_t)blockIdx.y * natom + start + ai] = make_double4(fx, fy, fz, en);
+    if (active) sr[(size_t)by * natom + start + ai] = make_double4(fx, fy, fz, en);
   }
+}
+
+__global__ void __launch_bounds__(kSrThreads)
+k_short_range(const double4 *__restrict__ pd, const uint32_t *__restrict__ cell_count,
+              const uint32_t *__restrict__ cell_point, Grid g, uint32_t natom,
+              double4 *__restrict__ sr) {
+  sr_block(pd, cell_count, cell_point, g, natom, sr, blockIdx.x, blockIdx.y);
 }
 
 // ----------------------------------------------------------------------------
@@ -1141,15 +1202,17 @@ constexpr int kCombineThreads = 256;
 constexpr int kCombineAtoms = 32;
 constexpr int kCombineWarps = kCombineThreads / 32;
 
-__global__ void __launch_bounds__(kCombineThreads)
-k_combine(const double4 *__restrict__ sr, const double4 *__restrict__ part, uint32_t nsplit,
-          const uint32_t *__restrict__ sorted_idx, uint32_t natom, int use_far,
-          double *__restrict__ cfx, double *__restrict__ cfy, double *__restrict__ cfz,
-          double *__restrict__ cen, double *__restrict__ ofx, double *__restrict__ ofy,
-          double *__restrict__ ofz, double *__restrict__ oen, double *__restrict__ block_energy) {
+__device__ __forceinline__ void combine_block(const double4 *__restrict__ sr, const double4 *__restrict__ part,
+                                              uint32_t nsplit, const uint32_t *__restrict__ sorted_idx,
+                                              uint32_t natom, int use_far, double *__restrict__ cfx,
+                                              double *__restrict__ cfy, double *__restrict__ cfz,
+                                              double *__restrict__ cen, double *__restrict__ ofx,
+                                              double *__restrict__ ofy, double *__restrict__ ofz,
+                                              double *__restrict__ oen, double *__restrict__ block_energy,
+                                              uint32_t bx) {
   __shared__ double4 s_rows[kCombineWarps][kCombineAtoms];
   const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
-  const uint32_t p = blockIdx.x * kCombineAtoms + lane;
+  const uint32_t p = bx * kCombineAtoms + lane;
   const bool live = p < natom;
   double4 acc = make_double4(0., 0., 0., 0.);
   if (live && use_far) {
@@ -1179,7 +1242,17 @@ k_combine(const double4 *__restrict__ sr, const double4 *__restrict__ part, uint
     e = t.w;
   }
   for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
-  if (lane == 0) block_energy[blockIdx.x] = e;
+  if (lane == 0) block_energy[bx] = e;
+}
+
+__global__ void __launch_bounds__(kCombineThreads)
+k_combine(const double4 *__restrict__ sr, const double4 *__restrict__ part, uint32_t nsplit,
+          const uint32_t *__restrict__ sorted_idx, uint32_t natom, int use_far,
+          double *__restrict__ cfx, double *__restrict__ cfy, double *__restrict__ cfz,
+          double *__restrict__ cen, double *__restrict__ ofx, double *__restrict__ ofy,
+          double *__restrict__ ofz, double *__restrict__ oen, double *__restrict__ block_energy) {
+  combine_block(sr, part, nsplit, sorted_idx, natom, use_far, cfx, cfy, cfz, cen, ofx, ofy, ofz, oen, block_energy,
+                blockIdx.x);
 }
 
 // ----------------------------------------------------------------------------
@@ -1221,8 +1294,8 @@ k_reduce_shards(ShardSet ss, uint32_t natom, double *__restrict__ block_energy) 
 }
 
 // Total energy 0.5 * sum of the per-CTA sums, fixed order (one CTA).
-__global__ void k_energy_total(const double *__restrict__ block_energy, uint32_t nblocks,
-                               double *__restrict__ total) {
+__device__ __forceinline__ void energy_body(const double *__restrict__ block_energy, uint32_t nblocks,
+                                            double *__restrict__ total) {
   __shared__ double s_red[32];
   double e = 0.0;
   for (uint32_t b = threadIdx.x; b < nblocks; b += blockDim.x) e += block_energy[b];
@@ -1234,6 +1307,11 @@ __global__ void k_energy_total(const double *__restrict__ block_energy, uint32_t
     for (unsigned w = 0; w < (blockDim.x >> 5); w++) t += s_red[w];
     *total = 0.5 * t;
   }
+}
+
+__global__ void k_energy_total(const double *__restrict__ block_energy, uint32_t nblocks,
+                               double *__restrict__ total) {
+  energy_body(block_energy, nblocks, total);
 }
 
 // ----------------------------------------------------------------------------

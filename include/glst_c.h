@@ -275,11 +275,22 @@ glst_status glst_batch_create(glst_batch **out, uint32_t nsys,
                               uint32_t nstreams);
 glst_status glst_batch_destroy(glst_batch *b);
 
-/* Solve every system.  `plain` = 0: the captured graph (captured on the first
- * call and again whenever the pointers change); `plain` = 1: the systems one
- * after another on one stream, each its own launch sequence (the
- * one-system-per-launch baseline).  Outputs in input order per system.
- * Stream ordered. */
+/* Solve every system.  `plain` selects the schedule:
+ *   0: one captured CUDA graph (captured on the first call and again whenever
+ *      the pointers or the mode change) in which every system that fits the
+ *      work-list kernels (whole system, one node stage, shell sums in shared
+ *      memory) is solved by ONE persistent launch per phase -- assignment,
+ *      structure factors, shell sums, gather, near field, combine -- over a
+ *      work list of (system, unit / cell / node block / atom block x chunk)
+ *      items, each item running exactly the code the system's own launch
+ *      would; the other systems run their own launch sequences on parallel
+ *      graph branches beside it;
+ *   1: the systems one after another on one stream, each its own launch
+ *      sequence (the one-system-per-launch baseline);
+ *   2: one captured graph of every system's own launch sequence spread over
+ *      `nstreams` branches.
+ * Every mode gives every system bit for bit the result it gets alone.
+ * Outputs in input order per system.  Stream ordered. */
 glst_status glst_batch_compute(glst_batch *b, const double *d_rx,
                                const double *d_ry, const double *d_rz,
                                const double *d_qc, double *d_fx, double *d_fy,

@@ -17,6 +17,9 @@ def _cat(systems, key):
 
 
 def test_batch_equals_individual_solves(pkg):
+    """Ten uneven systems (a few without far field): the work-list graph, its
+    replay, the plain sequence and the branch graph all give every system
+    bit for bit its result alone."""
     from glst_b200 import systems as S
     sy = S.batch_uneven(10, seed=3, mol_min=100, mol_max=2500)
     ins = [_cat(sy, k) for k in ("x", "y", "z", "q")]
@@ -33,9 +36,14 @@ def test_batch_equals_individual_solves(pkg):
         b.compute(*ins, *outs, plain=True)     # one system after another
         torch.cuda.synchronize()
         plain = [o.cpu().numpy().copy() for o in outs]
+        b.compute(*ins, *outs, mode="branches")  # each system its own launches, graph branches
+        torch.cuda.synchronize()
+        branches = [o.cpu().numpy().copy() for o in outs]
+        e_branches = b.energies()
         off = b.offsets
-    for a, r, p in zip(graph, replay, plain):
-        assert np.array_equal(a, r) and np.array_equal(a, p)
+    for a, r, p, br in zip(graph, replay, plain, branches):
+        assert np.array_equal(a, r) and np.array_equal(a, p) and np.array_equal(a, br)
+    assert np.array_equal(e_graph, e_branches)
     for i, s in enumerate(sy):
         with pkg.GlstForce(s["natom"], s["tol"], *s["box"], rcut=s["rcut"]) as f:
             f.calc_ener_force(*[torch.tensor(s[k], dtype=torch.float64, device="cuda:0") for k in ("x", "y", "z", "q")])
