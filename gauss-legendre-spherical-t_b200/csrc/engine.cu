@@ -1419,15 +1419,22 @@ struct glst_batch {
   double *energies = nullptr;           // device, one per system
   // Work list: systems solved by one persistent launch per phase (the rest
   // keep their own launch sequences on the other branches).
-  std::vector<uint32_t> wl;             // batch indices of the work-list systems
+  std::vector<uint32_t> wl;             // batch indices of the work-list systems (descriptor order)
   std::vector<uint8_t> in_wl;           // per system
   enum { kZero, kBin, kScan, kScatter, kSort, kSf, kShell, kLr, kSr, kCombine, kEnergy, kPhases };
-  uint32_t ph_off[kPhases] = {}, ph_n[kPhases] = {}, ph_grid[kPhases] = {};
+  // The work-list systems form `groups` work lists, each launched on its own
+  // graph branch, so that phases of different groups overlap (the SFU-bound
+  // structure factors of one group beside the shared-memory-bound shell sums
+  // of another).
+  struct WlGroup {
+    uint32_t ph_off[kPhases] = {}, ph_n[kPhases] = {}, ph_grid[kPhases] = {};
+    size_t shell_smem = 0;              // dynamic shared memory of the shell-sum launch
+    cudaStream_t side = nullptr;        // near field beside the far field
+    cudaEvent_t fork = nullptr, join = nullptr;
+  };
+  std::vector<WlGroup> groups;
   dev::WorkItem *d_items = nullptr;
   dev::SysDesc *d_desc = nullptr;
-  size_t shell_smem = 0;                // dynamic shared memory of the shell-sum launch
-  cudaStream_t wl_side = nullptr;       // near field of the work list, beside its far field
-  cudaEvent_t wl_fork = nullptr, wl_join = nullptr;
 };
 
 static constexpr uint32_t kBatchLargeAtoms = 20000;  // fills the GPU by itself
@@ -1455,16 +1462,17 @@ static void batch_release(glst_batch *b) {
   if (b->energies) cudaFree(b->energies);
   if (b->d_items) cudaFree(b->d_items);
   if (b->d_desc) cudaFree(b->d_desc);
-  if (b->wl_side) cudaStreamDestroy(b->wl_side);
-  if (b->wl_fork) cudaEventDestroy(b->wl_fork);
-  if (b->wl_join) cudaEventDestroy(b->wl_join);
+  for (auto &gr : b->groups) {
+    if (gr.side) cudaStreamDestroy(gr.side);
+    if (gr.fork) cudaEventDestroy(gr.fork);
+    if (gr.join) cudaEventDestroy(gr.join);
+  }
+  b->groups.clear();
   b->own = nullptr;
   b->ev_in = b->ev_out = nullptr;
   b->energies = nullptr;
   b->d_items = nullptr;
   b->d_desc = nullptr;
-  b->wl_side = nullptr;
-  b->wl_fork = b->wl_join = nullptr;
 }
 
 // A system joins the work list when its solve is one launch of each kernel
@@ -1477,104 +1485,132 @@ static bool worklist_ok(const glst_handle *h) {
   return true;
 }
 
-// Work items of every phase for the work-list systems, and the persistent
-// grid of each phase's kernel (resident CTAs on every SM, at most one per item).
-static glst_status worklist_build(glst_batch *b) {
+// Work items of every phase for the work-list systems, split into groups
+// (systems dealt largest first to the least loaded group), and each phase
+// kernel's grid: one CTA per item, or -- GLST_WORKLIST_GRID=persistent when a
+// batch is created -- resident CTAs on every SM taking the items in a
+// stride.  GLST_WORKLIST_GROUPS sets the number of groups (default 4, at
+// most the batch's branches).
+static glst_status worklist_build(glst_batch *b, const std::vector<double> &cost) {
   b->wl.clear();
   b->in_wl.assign(b->sys.size(), 0);
-  for (uint32_t i = 0; i < b->sys.size(); i++)
-    if (worklist_ok(b->sys[i])) {
-      b->wl.push_back(i);
-      b->in_wl[i] = 1;
+  std::vector<uint32_t> cand;
+  for (uint32_t i : b->order)  // largest estimated cost first
+    if (worklist_ok(b->sys[i])) cand.push_back(i);
+  if (cand.empty()) return GLST_OK;
+  uint32_t ng = 4;
+  if (const char *e = std::getenv("GLST_WORKLIST_GROUPS")) ng = (uint32_t)std::max(1, std::atoi(e));
+  ng = std::max<uint32_t>(1, std::min<uint32_t>({ng, (uint32_t)b->branch.size(), (uint32_t)cand.size()}));
+  const char *ge = std::getenv("GLST_WORKLIST_GRID");
+  const bool persistent = ge && std::string(ge) == "persistent";
+  std::vector<std::vector<uint32_t>> members(ng);
+  {
+    std::vector<double> load(ng, 0.0);
+    for (uint32_t i : cand) {
+      const uint32_t gsel = (uint32_t)(std::min_element(load.begin(), load.end()) - load.begin());
+      members[gsel].push_back(i);
+      load[gsel] += cost[i];
     }
-  if (b->wl.empty()) return GLST_OK;
-  std::vector<dev::WorkItem> items;
-  auto begin = [&](int ph) { b->ph_off[ph] = (uint32_t)items.size(); };
-  auto end = [&](int ph) { b->ph_n[ph] = (uint32_t)items.size() - b->ph_off[ph]; };
-  const uint32_t nw = (uint32_t)b->wl.size();
-  auto each = [&](int ph, auto &&fn) {
-    begin(ph);
-    for (uint32_t w = 0; w < nw; w++) fn(w, b->sys[b->wl[w]]);
-    end(ph);
-  };
-  each(glst_batch::kZero, [&](uint32_t w, glst_handle *h) {
-    for (uint32_t c = 0; c < (h->plan.ncell + 1023) / 1024; c++) items.push_back({w, c, 0, 0});
-  });
-  each(glst_batch::kBin, [&](uint32_t w, glst_handle *h) {
-    for (uint32_t a = 0; a < (h->plan.natom + 255) / 256; a++) items.push_back({w, a, 0, 0});
-  });
-  each(glst_batch::kScan, [&](uint32_t w, glst_handle *) { items.push_back({w, 0, 0, 0}); });
-  each(glst_batch::kScatter, [&](uint32_t w, glst_handle *h) {
-    for (uint32_t a = 0; a < (h->plan.natom + 255) / 256; a++) items.push_back({w, a, 0, 0});
-  });
-  each(glst_batch::kSort, [&](uint32_t w, glst_handle *h) {
-    if (h->plan.natom)
-      for (uint32_t c = 0; c < h->plan.ncell; c++) items.push_back({w, c, 0, 0});
-  });
-  each(glst_batch::kSf, [&](uint32_t w, glst_handle *h) {
-    if (!h->K || !h->plan.natom) return;
-    const uint32_t rows = (h->plan.ncell + dev::kSfCellsPerCta - 1) / dev::kSfCellsPerCta;
-    for (uint32_t r = 0; r < rows; r++)
-      for (uint32_t u = 0; u < h->n_sf_units; u++) items.push_back({w, u, r, 0});
-  });
-  each(glst_batch::kShell, [&](uint32_t w, glst_handle *h) {
-    if (!h->K || !h->plan.natom) return;
-    for (uint32_t k = 0; k < (h->K + h->sat_nb - 1) / h->sat_nb; k++) items.push_back({w, k, 0, 0});
-  });
-  each(glst_batch::kLr, [&](uint32_t w, glst_handle *h) {
-    if (!h->K || !h->plan.natom) return;
-    const uint32_t ab = (h->plan.natom + dev::kLrThreads - 1) / dev::kLrThreads;
-    for (uint32_t c = 0; c < h->nsplit; c++)
-      for (uint32_t a = 0; a < ab; a++) items.push_back({w, a, c, 0});
-  });
-  each(glst_batch::kSr, [&](uint32_t w, glst_handle *h) {
-    if (!h->plan.natom) return;
-    for (uint32_t pl = 0; pl < (uint32_t)dev::kSrPlanes; pl++)
-      for (uint32_t c = 0; c < h->plan.ncell; c++) items.push_back({w, c, pl, 0});
-  });
-  each(glst_batch::kCombine, [&](uint32_t w, glst_handle *h) {
-    if (h->plan.natom)
-      for (uint32_t a = 0; a < h->combine_blocks; a++) items.push_back({w, a, 0, 0});
-  });
-  each(glst_batch::kEnergy, [&](uint32_t w, glst_handle *) { items.push_back({w, 0, 0, 0}); });
-  CUDA_TRY(cudaMalloc(&b->d_items, std::max<size_t>(1, items.size()) * sizeof(dev::WorkItem)));
-  CUDA_TRY(cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(dev::WorkItem), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMalloc(&b->d_desc, nw * sizeof(dev::SysDesc)));
-  // shell sums: the largest work-list system's shared memory
-  b->shell_smem = 0;
-  for (uint32_t i : b->wl) {
-    const glst_handle *h = b->sys[i];
-    if (!h->K) continue;
-    const bool table = h->sat_xyz && h->sat_nb > 1;
-    b->shell_smem = std::max(b->shell_smem, h->sat_per_node * h->sat_nb +
-                                                (table ? (((size_t)h->plan.ncell * 4 + 15) & ~size_t(15)) : 0));
   }
+  for (auto &m : members)
+    for (uint32_t i : m) {
+      b->in_wl[i] = 1;
+      b->wl.push_back(i);  // descriptor index = position in wl
+    }
+  b->groups.assign(ng, glst_batch::WlGroup{});
+  std::vector<dev::WorkItem> items;
   int nsm = 148, smem_optin = 0;
   CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device));
   CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device));
   CUDA_TRY(cudaFuncSetAttribute(dev::k_shell_sums_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_optin));
   CUDA_TRY(cudaFuncSetAttribute(dev::k_sort_pack_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(dev::kSortCap * sizeof(uint32_t))));
-  auto grid = [&](int ph, const void *fn, int threads, size_t smem) -> glst_status {
-    int per_sm = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
-    b->ph_grid[ph] = std::max<uint32_t>(1, std::min<uint32_t>(b->ph_n[ph], (uint32_t)std::max(1, per_sm) * nsm));
-    return GLST_OK;
-  };
-  GLST_TRY(grid(glst_batch::kZero, (const void *)dev::k_zero_counts_multi, 1024, 0));
-  GLST_TRY(grid(glst_batch::kBin, (const void *)dev::k_bin_multi, 256, 0));
-  GLST_TRY(grid(glst_batch::kScan, (const void *)dev::k_scan_multi, 1024, 0));
-  GLST_TRY(grid(glst_batch::kScatter, (const void *)dev::k_scatter_multi, 256, 0));
-  GLST_TRY(grid(glst_batch::kSort, (const void *)dev::k_sort_pack_multi, 256, dev::kSortCap * sizeof(uint32_t)));
-  GLST_TRY(grid(glst_batch::kSf, (const void *)dev::k_structure_factors_multi, dev::kSfThreads, 0));
-  GLST_TRY(grid(glst_batch::kShell, (const void *)dev::k_shell_sums_multi, dev::kSatThreads, b->shell_smem));
-  GLST_TRY(grid(glst_batch::kLr, (const void *)dev::k_long_range_multi, dev::kLrThreads, 0));
-  GLST_TRY(grid(glst_batch::kSr, (const void *)dev::k_short_range_multi, dev::kSrThreads, 0));
-  GLST_TRY(grid(glst_batch::kCombine, (const void *)dev::k_combine_multi, dev::kCombineThreads, 0));
-  GLST_TRY(grid(glst_batch::kEnergy, (const void *)dev::k_energy_multi, 256, 0));
-  CUDA_TRY(cudaStreamCreateWithFlags(&b->wl_side, cudaStreamNonBlocking));
-  CUDA_TRY(cudaEventCreateWithFlags(&b->wl_fork, cudaEventDisableTiming));
-  CUDA_TRY(cudaEventCreateWithFlags(&b->wl_join, cudaEventDisableTiming));
+  uint32_t w0 = 0;
+  for (uint32_t gi = 0; gi < ng; gi++) {
+    glst_batch::WlGroup &gr = b->groups[gi];
+    const uint32_t nw = (uint32_t)members[gi].size();
+    auto each = [&](int ph, auto &&fn) {
+      gr.ph_off[ph] = (uint32_t)items.size();
+      for (uint32_t w = w0; w < w0 + nw; w++) fn(w, b->sys[b->wl[w]]);
+      gr.ph_n[ph] = (uint32_t)items.size() - gr.ph_off[ph];
+    };
+    each(glst_batch::kZero, [&](uint32_t w, glst_handle *h) {
+      for (uint32_t c = 0; c < (h->plan.ncell + 1023) / 1024; c++) items.push_back({w, c, 0, 0});
+    });
+    each(glst_batch::kBin, [&](uint32_t w, glst_handle *h) {
+      for (uint32_t a = 0; a < (h->plan.natom + 255) / 256; a++) items.push_back({w, a, 0, 0});
+    });
+    each(glst_batch::kScan, [&](uint32_t w, glst_handle *) { items.push_back({w, 0, 0, 0}); });
+    each(glst_batch::kScatter, [&](uint32_t w, glst_handle *h) {
+      for (uint32_t a = 0; a < (h->plan.natom + 255) / 256; a++) items.push_back({w, a, 0, 0});
+    });
+    each(glst_batch::kSort, [&](uint32_t w, glst_handle *h) {
+      if (h->plan.natom)
+        for (uint32_t c = 0; c < h->plan.ncell; c++) items.push_back({w, c, 0, 0});
+    });
+    each(glst_batch::kSf, [&](uint32_t w, glst_handle *h) {
+      if (!h->K || !h->plan.natom) return;
+      const uint32_t rows = (h->plan.ncell + dev::kSfCellsPerCta - 1) / dev::kSfCellsPerCta;
+      for (uint32_t r = 0; r < rows; r++)
+        for (uint32_t u = 0; u < h->n_sf_units; u++) items.push_back({w, u, r, 0});
+    });
+    each(glst_batch::kShell, [&](uint32_t w, glst_handle *h) {
+      if (!h->K || !h->plan.natom) return;
+      for (uint32_t k = 0; k < (h->K + h->sat_nb - 1) / h->sat_nb; k++) items.push_back({w, k, 0, 0});
+    });
+    each(glst_batch::kLr, [&](uint32_t w, glst_handle *h) {
+      if (!h->K || !h->plan.natom) return;
+      const uint32_t ab = (h->plan.natom + dev::kLrThreads - 1) / dev::kLrThreads;
+      for (uint32_t c = 0; c < h->nsplit; c++)
+        for (uint32_t a = 0; a < ab; a++) items.push_back({w, a, c, 0});
+    });
+    each(glst_batch::kSr, [&](uint32_t w, glst_handle *h) {
+      if (!h->plan.natom) return;
+      for (uint32_t pl = 0; pl < (uint32_t)dev::kSrPlanes; pl++)
+        for (uint32_t c = 0; c < h->plan.ncell; c++) items.push_back({w, c, pl, 0});
+    });
+    each(glst_batch::kCombine, [&](uint32_t w, glst_handle *h) {
+      if (h->plan.natom)
+        for (uint32_t a = 0; a < h->combine_blocks; a++) items.push_back({w, a, 0, 0});
+    });
+    each(glst_batch::kEnergy, [&](uint32_t w, glst_handle *) { items.push_back({w, 0, 0, 0}); });
+    // shell sums: the group's largest shared-memory need
+    for (uint32_t w = w0; w < w0 + nw; w++) {
+      const glst_handle *h = b->sys[b->wl[w]];
+      if (!h->K) continue;
+      const bool table = h->sat_xyz && h->sat_nb > 1;
+      gr.shell_smem = std::max(gr.shell_smem, h->sat_per_node * h->sat_nb +
+                                                  (table ? (((size_t)h->plan.ncell * 4 + 15) & ~size_t(15)) : 0));
+    }
+    auto grid = [&](int ph, const void *fn, int threads, size_t smem) -> glst_status {
+      uint32_t g = gr.ph_n[ph];
+      if (persistent) {
+        int per_sm = 0;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+        g = std::min<uint32_t>(g, (uint32_t)std::max(1, per_sm) * nsm);
+      }
+      gr.ph_grid[ph] = std::max<uint32_t>(1, g);
+      return GLST_OK;
+    };
+    GLST_TRY(grid(glst_batch::kZero, (const void *)dev::k_zero_counts_multi, 1024, 0));
+    GLST_TRY(grid(glst_batch::kBin, (const void *)dev::k_bin_multi, 256, 0));
+    GLST_TRY(grid(glst_batch::kScan, (const void *)dev::k_scan_multi, 1024, 0));
+    GLST_TRY(grid(glst_batch::kScatter, (const void *)dev::k_scatter_multi, 256, 0));
+    GLST_TRY(grid(glst_batch::kSort, (const void *)dev::k_sort_pack_multi, 256, dev::kSortCap * sizeof(uint32_t)));
+    GLST_TRY(grid(glst_batch::kSf, (const void *)dev::k_structure_factors_multi, dev::kSfThreads, 0));
+    GLST_TRY(grid(glst_batch::kShell, (const void *)dev::k_shell_sums_multi, dev::kSatThreads, gr.shell_smem));
+    GLST_TRY(grid(glst_batch::kLr, (const void *)dev::k_long_range_multi, dev::kLrThreads, 0));
+    GLST_TRY(grid(glst_batch::kSr, (const void *)dev::k_short_range_multi, dev::kSrThreads, 0));
+    GLST_TRY(grid(glst_batch::kCombine, (const void *)dev::k_combine_multi, dev::kCombineThreads, 0));
+    GLST_TRY(grid(glst_batch::kEnergy, (const void *)dev::k_energy_multi, 256, 0));
+    CUDA_TRY(cudaStreamCreateWithFlags(&gr.side, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&gr.fork, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&gr.join, cudaEventDisableTiming));
+    w0 += nw;
+  }
+  CUDA_TRY(cudaMalloc(&b->d_items, std::max<size_t>(1, items.size()) * sizeof(dev::WorkItem)));
+  CUDA_TRY(cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(dev::WorkItem), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMalloc(&b->d_desc, b->wl.size() * sizeof(dev::SysDesc)));
   return GLST_OK;
 }
 
@@ -1620,14 +1656,13 @@ static glst_status worklist_descriptors(glst_batch *b, const double *const in[4]
   return GLST_OK;
 }
 
-// The work-list solve on stream st: one launch per phase for all its systems;
-// the near field on a side stream beside the far field.
-static glst_status worklist_launch(glst_batch *b, cudaStream_t st) {
+// One group's work-list solve on stream st: one launch per phase for all its
+// systems; the near field on a side stream beside the far field.
+static glst_status worklist_launch(glst_batch *b, glst_batch::WlGroup &gr, cudaStream_t st) {
   const dev::SysDesc *D = b->d_desc;
-  auto it = [&](int ph) { return b->d_items + b->ph_off[ph]; };
   auto go = [&](int ph, auto kern, int threads, size_t smem, cudaStream_t s) -> glst_status {
-    if (!b->ph_n[ph]) return GLST_OK;
-    kern<<<b->ph_grid[ph], threads, smem, s>>>(D, it(ph), b->ph_n[ph]);
+    if (!gr.ph_n[ph]) return GLST_OK;
+    kern<<<gr.ph_grid[ph], threads, smem, s>>>(D, b->d_items + gr.ph_off[ph], gr.ph_n[ph]);
     CUDA_TRY(cudaGetLastError());
     return GLST_OK;
   };
@@ -1638,13 +1673,13 @@ static glst_status worklist_launch(glst_batch *b, cudaStream_t st) {
   GLST_TRY(go(glst_batch::kSort, dev::k_sort_pack_multi, 256, dev::kSortCap * sizeof(uint32_t), st));
   GLST_TRY(go(glst_batch::kSf, dev::k_structure_factors_multi, dev::kSfThreads, 0, st));
   // near field forked after the structure factors, as in a single solve
-  CUDA_TRY(cudaEventRecord(b->wl_fork, st));
-  CUDA_TRY(cudaStreamWaitEvent(b->wl_side, b->wl_fork, 0));
-  GLST_TRY(go(glst_batch::kSr, dev::k_short_range_multi, dev::kSrThreads, 0, b->wl_side));
-  CUDA_TRY(cudaEventRecord(b->wl_join, b->wl_side));
-  GLST_TRY(go(glst_batch::kShell, dev::k_shell_sums_multi, dev::kSatThreads, b->shell_smem, st));
+  CUDA_TRY(cudaEventRecord(gr.fork, st));
+  CUDA_TRY(cudaStreamWaitEvent(gr.side, gr.fork, 0));
+  GLST_TRY(go(glst_batch::kSr, dev::k_short_range_multi, dev::kSrThreads, 0, gr.side));
+  CUDA_TRY(cudaEventRecord(gr.join, gr.side));
+  GLST_TRY(go(glst_batch::kShell, dev::k_shell_sums_multi, dev::kSatThreads, gr.shell_smem, st));
   GLST_TRY(go(glst_batch::kLr, dev::k_long_range_multi, dev::kLrThreads, 0, st));
-  CUDA_TRY(cudaStreamWaitEvent(st, b->wl_join, 0));
+  CUDA_TRY(cudaStreamWaitEvent(st, gr.join, 0));
   GLST_TRY(go(glst_batch::kCombine, dev::k_combine_multi, dev::kCombineThreads, 0, st));
   GLST_TRY(go(glst_batch::kEnergy, dev::k_energy_multi, 256, 0, st));
   return GLST_OK;
@@ -1678,14 +1713,16 @@ static glst_status batch_capture(glst_batch *b, const double *const in[4], doubl
   glst_status s = GLST_OK;
   cudaError_t e = cudaEventRecord(b->ev_in, b->own);
   for (size_t j = 0; e == cudaSuccess && j < b->branch.size(); j++) e = cudaStreamWaitEvent(b->branch[j], b->ev_in, 0);
-  if (e == cudaSuccess && wl) s = worklist_launch(b, b->branch[0]);
   const size_t nbr = b->branch.size();
-  size_t next = 0;  // round robin over branches 1.. for the others in work-list mode
+  const size_t ng = wl ? b->groups.size() : 0;  // groups on branches 0 .. ng-1
+  for (size_t gi = 0; e == cudaSuccess && s == GLST_OK && gi < ng; gi++)
+    s = worklist_launch(b, b->groups[gi], b->branch[gi]);
+  size_t next = 0;  // round robin over the branches after the groups' for the others
   for (size_t t = 0; e == cudaSuccess && s == GLST_OK && t < b->order.size(); t++) {
     const uint32_t i = b->order[t];
     if (wl && b->in_wl[i]) continue;
     cudaStream_t st = b->branch[b->branch_of[i]];
-    if (wl) st = b->branch[nbr > 1 ? 1 + (next++ % (nbr - 1)) : 0];
+    if (wl) st = b->branch[nbr > ng ? ng + (next++ % (nbr - ng)) : (next++ % nbr)];
     s = batch_one(b, i, in, out, st);
   }
   for (size_t j = 0; e == cudaSuccess && j < b->branch.size(); j++) {
@@ -1773,7 +1810,7 @@ glst_status glst_batch_create(glst_batch **out, uint32_t nsys, const uint32_t *n
   CUDA_TRY(cudaMalloc(&b->energies, sizeof(double) * std::max<uint32_t>(1, nsys)));
   CUDA_TRY(cudaMemset(b->energies, 0, sizeof(double) * std::max<uint32_t>(1, nsys)));
   {
-    const glst_status ws = worklist_build(b.get());
+    const glst_status ws = worklist_build(b.get(), cost);
     if (ws != GLST_OK) {
       batch_release(b.get());
       return ws;
