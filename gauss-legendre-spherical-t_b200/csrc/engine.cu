@@ -114,6 +114,8 @@ struct glst_handle {
   uint32_t shard = 0, nshards = 1;  // node split across devices (1 = whole system)
   uint32_t k_begin = 0;             // first node (internal order) of this shard
   uint32_t lr_waves = 8;            // long-range CTAs ~ lr_waves x resident slots
+  uint32_t lr_variant = 0;          // gather's FMA-pipe sin/cos share (kLrPolyMasks)
+  uint32_t sf_max_npt = dev::kSfMaxNpt;  // radial nodes per thread, at most, in the structure-factor units
   size_t part_cap = 0;              // rows the part buffer holds
   size_t sat_per_node = 0;          // shell-sum shared bytes per node
   size_t sat_budget = 0;            // shell-sum shared bytes per CTA, at most
@@ -280,6 +282,7 @@ static void release(glst_handle *h, bool device_idle = false) {
 // bucket) for every later handle of that shape in this process.
 struct Tuning {
   uint32_t sat_nb = 0, lr_waves = 0;  // 0 = default
+  uint32_t lr_variant = 0, sf_max_npt = 0;
 };
 static std::mutex g_tune_mu;
 static std::map<std::tuple<uint32_t, uint32_t, uint32_t>, Tuning> g_tune;
@@ -423,7 +426,7 @@ static glst_status build_chunks(glst_handle *h, bool in_arena = false) {
       // kSfThreads / nb directions, nb threads per direction of npt <=
       // kSfMaxNpt radial nodes (cutting the whole run, not each chunk, keeps
       // the units full).
-      const uint32_t nb = (g.n_radial + dev::kSfMaxNpt - 1) / dev::kSfMaxNpt;
+      const uint32_t nb = (g.n_radial + h->sf_max_npt - 1) / h->sf_max_npt;
       const uint32_t npt = (g.n_radial + nb - 1) / nb;
       const uint32_t dpu = dev::kSfThreads / nb;
       for (uint32_t j0 = 0; j0 < n_dir; j0 += dpu) {
@@ -616,11 +619,10 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
     int smem_optin = 0, nsm = 148;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
     CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
-    // row = a node's prefix table with a zero plane in front along each
-    // axis; row stride = 1 (mod 8) complex doubles: rows of consecutive nodes
-    // start 16 bytes apart modulo 128, so the node-fastest accesses of the
-    // shell pass spread over all shared-memory banks
-    h->sat_stride = dev::sat_padded_cells(p.n[0], p.n[1], p.n[2]);
+    // row stride = 1 (mod 8) complex doubles: rows of consecutive nodes start
+    // 16 bytes apart modulo 128, so the node-fastest accesses of the shell
+    // pass spread over all shared-memory banks
+    h->sat_stride = (uint32_t)(C + 1);
     while (h->sat_stride % 8 != 1) h->sat_stride++;
     const size_t per_node = ((size_t)h->sat_stride + p.n[0] + p.n[1] + p.n[2]) * sizeof(double2);
     // the cell-coordinate table (4 bytes per cell) comes off the budget when
@@ -645,6 +647,8 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
       if (t.sat_nb && !h->gsat)
         h->sat_nb = pow2_floor(std::min<uint32_t>(t.sat_nb, (uint32_t)std::max<size_t>(1, budget / per_node)));
       if (t.lr_waves) h->lr_waves = t.lr_waves;
+      h->lr_variant = t.lr_variant;
+      if (t.sf_max_npt) h->sf_max_npt = t.sf_max_npt;
     }
     GLST_TRY(build_chunks(h, /*in_arena=*/true));
     const size_t kpad = ((size_t)h->stage_kmax + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock;
@@ -776,9 +780,18 @@ static glst_status lr_stage(glst_handle *h, size_t stage, cudaStream_t st) {
   if (rg.c1 <= rg.c0 || !h->plan.natom) return GLST_OK;
   dim3 grid((h->plan.natom + dev::kLrThreads - 1) / dev::kLrThreads, rg.c1 - rg.c0);
   // stage 0 writes its rows, later stages add into the same rows
-  dev::k_long_range_flat<<<grid, dev::kLrThreads, 0, st>>>(
-      h->pk, h->cell_point, h->plan.ncell, h->chunks + rg.c0, h->dirs, h->kappa, h->R, rg.kb, h->plan.natom,
-      stage > 0 ? 1 : 0, h->part);
+#define GLST_LR(v)                                                                                            \
+  case v:                                                                                                     \
+    dev::k_long_range_flat<v><<<grid, dev::kLrThreads, 0, st>>>(h->pk, h->cell_point, h->plan.ncell,          \
+                                                                h->chunks + rg.c0, h->dirs, h->kappa, h->R,   \
+                                                                rg.kb, h->plan.natom, stage > 0 ? 1 : 0,      \
+                                                                h->part);                                     \
+    break;
+  switch (h->lr_variant) {
+    GLST_LR(0) GLST_LR(1) GLST_LR(2) GLST_LR(3)
+    default: return fail(GLST_ERR_INVALID_ARG, "bad gather variant");
+  }
+#undef GLST_LR
   CUDA_TRY(cudaGetLastError());
   return GLST_OK;
 }
@@ -1130,6 +1143,8 @@ glst_status glst_get_info(const glst_handle *h, glst_info *info) {
   info->kernels_per_compute = h->plan.natom ? 4u + (h->shard == 0 ? 1u : 0u) + far + 2u : 2u;
   info->node_stages = (uint32_t)h->ranges.size();
   info->shell_sums_global = h->gsat ? 1u : 0u;
+  info->gather_variant = h->lr_variant;
+  info->sf_max_npt = h->sf_max_npt;
   return GLST_OK;
 }
 
@@ -1216,10 +1231,32 @@ glst_status glst_autotune(glst_handle *h, const double *rx, const double *ry, co
     }
     h->lr_waves = best_w;
     GLST_TRY(build_chunks(h));
+    // long-range gather: FMA-pipe sine/cosine share (compiled variants)
+    uint32_t best_v = h->lr_variant;
+    best = 1e30f;
+    for (uint32_t v = 0; v < (uint32_t)dev::kLrVariants; v++) {
+      h->lr_variant = v;
+      float ms = 0.f;
+      GLST_TRY(timed(phase_lr, &ms));
+      if (ms < best) best = ms, best_v = v;
+    }
+    h->lr_variant = best_v;
+    // structure factors: radial nodes per thread, at most (units' shape)
+    uint32_t best_npt = h->sf_max_npt;
+    best = 1e30f;
+    for (uint32_t npt : {12u, 8u, 6u}) {
+      h->sf_max_npt = npt;
+      GLST_TRY(build_chunks(h));
+      float ms = 0.f;
+      GLST_TRY(timed(phase_sf, &ms));
+      if (ms < best) best = ms, best_npt = npt;
+    }
+    h->sf_max_npt = best_npt;
+    GLST_TRY(build_chunks(h));
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune[tune_key(h->plan, h->K)] = Tuning{h->sat_nb, h->lr_waves};
+    g_tune[tune_key(h->plan, h->K)] = Tuning{h->sat_nb, h->lr_waves, h->lr_variant, h->sf_max_npt};
   }
   if (sat_nb) *sat_nb = h->sat_nb;
   if (lr_waves) *lr_waves = h->lr_waves;
@@ -1480,6 +1517,7 @@ static void batch_release(glst_batch *b) {
 // shell sums in shared memory with several nodes per CTA (or no far field).
 static bool worklist_ok(const glst_handle *h) {
   if (h->nshards != 1 || h->ranges.size() > 1 || h->gsat) return false;
+  if (h->lr_variant != 0) return false;  // the work-list gather is the default variant
   if (h->K && h->sat_nb < 2) return false;
   if ((h->plan.ncell + dev::kSfCellsPerCta - 1) / dev::kSfCellsPerCta > 65535u) return false;
   return true;

@@ -515,12 +515,12 @@ k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ 
 // R_c = w * [box(c, r_out) - box(c, r_in)], 8 corners per box, clipped to the
 // grid.  All FP64.  Output R'_c(k) = R_c(k) e^{+ik.c} as float2, the twiddle
 // built from per-axis tables e^{i kx cx} e^{i ky cy} e^{i kz cz}.
-// The prefix table of a node is held with one zero plane in front along
-// every axis ((nx+1) x (ny+1) x (nz+1) entries, entry (X, Y, Z) = sum over
-// cells x < X, y < Y, z < Z): a box's corners are at offsets X*sx + Y*sy + Z
-// built from two values per axis, and a corner in a zero plane is simply not
-// loaded.
-// CTA: nb nodes at once (rows of `stride` complex doubles in shared memory).
+// CTA: nb nodes at once (rows of ncell+1 complex doubles in shared memory).
+// (A form with a zero plane in front of each axis, so that corner offsets
+// need no clipping tests, measured slower on water10k: 0.50 ms loading all
+// eight corners of every box, 0.45 ms skipping the zero-plane corners,
+// against 0.42 ms here -- the larger rows and their zeroing cost more than
+// the index arithmetic saved.)
 constexpr int kSatThreads = 512;
 constexpr int kSatThreadsOne = 1024;  // one node per CTA (large grids): more warps per SM
 constexpr int kSatLoadBatch = 4;
@@ -534,45 +534,39 @@ struct SatArgs {
   uint32_t nb;                  // nodes per CTA (a power of two, <= 32)
   uint32_t lg_nb;               // log2(nb)
   uint32_t xyz_table;           // 1: cell coordinates tabulated in shared memory
-  uint32_t stride;              // shared row stride (complex), >= padded table size, = 1 (mod 8)
+  uint32_t stride;              // shared row stride (complex), >= ncell, = 1 (mod 8)
   float2 *R;
 };
 
-// Entries of a node's padded prefix table.
-__host__ __device__ __forceinline__ uint32_t sat_padded_cells(uint32_t nx, uint32_t ny, uint32_t nz) {
-  return (nx + 1) * (ny + 1) * (nz + 1);
+__device__ __forceinline__ double2 sat_at(const double2 *row, uint32_t x, uint32_t y,
+                                          uint32_t z, const Grid &g) {
+  return row[(x * g.ny + y) * g.nz + z];
+}
+
+__device__ __forceinline__ double2 cube_sum(const double2 *row, uint32_t x, uint32_t y,
+                                            uint32_t z, uint32_t r, const Grid &g) {
+  const uint32_t x0 = (x < r) ? 0 : x - r, y0 = (y < r) ? 0 : y - r, z0 = (z < r) ? 0 : z - r;
+  const uint32_t x1 = min(x + r, g.nx - 1), y1 = min(y + r, g.ny - 1), z1 = min(z + r, g.nz - 1);
+  const bool xb = x0 == 0, yb = y0 == 0, zb = z0 == 0;
+  const uint32_t xm = xb ? 0 : x0 - 1, ym = yb ? 0 : y0 - 1, zm = zb ? 0 : z0 - 1;
+  double2 s = sat_at(row, x1, y1, z1, g);
+  double2 t;
+  if (!xb) { t = sat_at(row, xm, y1, z1, g); s.x -= t.x; s.y -= t.y; }
+  if (!yb) { t = sat_at(row, x1, ym, z1, g); s.x -= t.x; s.y -= t.y; }
+  if (!zb) { t = sat_at(row, x1, y1, zm, g); s.x -= t.x; s.y -= t.y; }
+  if (!xb && !yb) { t = sat_at(row, xm, ym, z1, g); s.x += t.x; s.y += t.y; }
+  if (!xb && !zb) { t = sat_at(row, xm, y1, zm, g); s.x += t.x; s.y += t.y; }
+  if (!yb && !zb) { t = sat_at(row, x1, ym, zm, g); s.x += t.x; s.y += t.y; }
+  if (!xb && !yb && !zb) { t = sat_at(row, xm, ym, zm, g); s.x -= t.x; s.y -= t.y; }
+  return s;
 }
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// Box sum of the cells [x0, x1] x [y0, y1] x [z0, z1] from the padded table:
-// the caller passes the corner coordinates already scaled by the strides:
-// xl = x0 * sx, xh = (x1 + 1) * sx, likewise y with sy, z unscaled.  The eight
-// terms are added in the order of the reference's box_sum
-// (src/glst_force.cu:774-845).  A low corner in the zero plane (xl, yl or zl
-// = 0) contributes zeros, so its loads are skipped: on small grids most boxes
-// are clipped, and loading all eight corners measured slower (water10k shell
-// sums 0.50 against 0.42 ms), the loads being the kernel's shared-memory
-// traffic.
-__device__ __forceinline__ double2 box_padded(const double2 *row, uint32_t xl, uint32_t xh, uint32_t yl,
-                                              uint32_t yh, uint32_t zl, uint32_t zh) {
-  const uint32_t hh = xh + yh, lh = xl + yh, hl = xh + yl, ll = xl + yl;
-  double2 s = row[hh + zh];
-  double2 t;
-  if (xl) { t = row[lh + zh]; s.x -= t.x; s.y -= t.y; }
-  if (yl) { t = row[hl + zh]; s.x -= t.x; s.y -= t.y; }
-  if (zl) { t = row[hh + zl]; s.x -= t.x; s.y -= t.y; }
-  if (xl && yl) { t = row[ll + zh]; s.x += t.x; s.y += t.y; }
-  if (xl && zl) { t = row[lh + zl]; s.x += t.x; s.y += t.y; }
-  if (yl && zl) { t = row[hl + zl]; s.x += t.x; s.y += t.y; }
-  if (xl && yl && zl) { t = row[ll + zl]; s.x -= t.x; s.y -= t.y; }
-  return s;
-}
-
-// Dynamic shared memory: nb rows of `stride` complex (the padded tables), the
-// twiddle tables nb x (nx + ny + nz) complex, then, in the several-nodes form
+// Dynamic shared memory: nb rows of `stride` complex (the SAT), the twiddle
+// tables nb x (nx + ny + nz) complex, then, in the several-nodes form
 // (kMinBlocks > 1, small grids) when it fits, the cell coordinates (ncell x
 // u32, x | y << 10 | z << 20).  nb is a power of two <= 32: lane l of a warp works
 // on node l % nb of the CTA and on the (l / nb)-th of the 32 / nb cells or
@@ -586,7 +580,6 @@ __device__ __forceinline__ void shell_block(const Grid &g, const SatArgs &a, uin
   const uint32_t k0 = bx * nb;
   const uint32_t C = g.ncell;
   const uint32_t naxis = g.nx + g.ny + g.nz;
-  const uint32_t sy = g.nz + 1, sx = (g.ny + 1) * sy;  // padded strides
   double2 *s_tw = s_sat + (size_t)nb * a.stride;
   uint32_t *s_xyz = reinterpret_cast<uint32_t *>(s_tw + (size_t)nb * naxis);
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -625,22 +618,6 @@ __device__ __forceinline__ void shell_block(const Grid &g, const SatArgs &a, uin
     sincos(kc, &sn, &cs);
     s_tw[t] = make_double2(cs, sn);
   }
-  // the zero planes X = 0 and Y = 0 of every row (the Z = 0 entries of the
-  // other lines are written by the load pass)
-  {
-    const uint32_t nxz = g.nx * sy;
-    for (uint32_t t = threadIdx.x; t < nb * (sx + nxz); t += blockDim.x) {
-      const uint32_t jj = t / (sx + nxz), r = t - jj * (sx + nxz);
-      uint32_t off;
-      if (r < sx) {
-        off = r;
-      } else {
-        const uint32_t q = r - sx, xq = q / sy;
-        off = (xq + 1) * sx + (q - xq * sy);
-      }
-      s_sat[(size_t)jj * a.stride + off] = zero;
-    }
-  }
   auto coords = [&](uint32_t c) {
     const uint32_t x = c / (g.ny * g.nz), rem = c - x * (g.ny * g.nz);
     const uint32_t y = rem / g.nz, z = rem - y * g.nz;
@@ -656,17 +633,15 @@ __device__ __forceinline__ void shell_block(const Grid &g, const SatArgs &a, uin
   // prefix pass without its own shared-memory round trip)
   {
     double2 acc = zero, txy = zero;
-    uint32_t base = 0;
     while (l < nlines) {
       uint32_t ln = l, zn = z0 + kSatLoadBatch;
       if (zn >= g.nz) { ln = l + step; zn = 0; }
       if (z0 == 0) {
-        const uint32_t lx = l / g.ny, ly = l - lx * g.ny;
-        txy = cmul(twx[lx], twy[ly]);  // e^{+i(kx cx + ky cy)}
+        const uint32_t lx = l / g.ny;
+        txy = cmul(twx[lx], twy[l - lx * g.ny]);  // e^{+i(kx cx + ky cy)}
         acc = zero;
-        base = (lx + 1) * sx + (ly + 1) * sy;  // padded line (x + 1, y + 1, .)
-        row[base] = zero;                      // its Z = 0 entry
       }
+      const uint32_t base = l * g.nz;
 #pragma unroll
       for (int u = 0; u < kSatLoadBatch; u++) {
         if (z0 + u < g.nz) {
@@ -674,7 +649,7 @@ __device__ __forceinline__ void shell_block(const Grid &g, const SatArgs &a, uin
           const double vx = v[u].x, vy = v[u].y;
           acc.x += vx * t.x + vy * t.y;  // v * conj(t)
           acc.y += vy * t.x - vx * t.y;
-          row[base + z0 + u + 1] = acc;
+          row[base + z0 + u] = acc;
         }
       }
       fetch(v, ln, zn);
@@ -686,17 +661,19 @@ __device__ __forceinline__ void shell_block(const Grid &g, const SatArgs &a, uin
   // prefix along y (lines x, z)
   for (uint32_t l = first; l < g.nx * g.nz; l += step) {
     const uint32_t x = l / g.nz, z = l - x * g.nz;
-    double2 *p = row + (x + 1) * sx + (z + 1);
-    double2 acc = zero;
-    for (uint32_t y = 1; y <= g.ny; y++) { acc.x += p[y * sy].x; acc.y += p[y * sy].y; p[y * sy] = acc; }
+    double2 *p = row + x * g.ny * g.nz + z;
+    double2 acc = make_double2(0.0, 0.0);
+    for (uint32_t y = 0; y < g.ny; y++) { acc.x += p[y * g.nz].x; acc.y += p[y * g.nz].y; p[y * g.nz] = acc; }
   }
   __syncthreads();
   // prefix along x (lines y, z)
-  for (uint32_t l = first; l < g.ny * g.nz; l += step) {
-    const uint32_t y = l / g.nz, z = l - y * g.nz;
-    double2 *p = row + (y + 1) * sy + (z + 1);
-    double2 acc = zero;
-    for (uint32_t x = 1; x <= g.nx; x++) { acc.x += p[x * sx].x; acc.y += p[x * sx].y; p[x * sx] = acc; }
+  {
+    const uint32_t sx = g.ny * g.nz;
+    for (uint32_t l = first; l < sx; l += step) {
+      double2 *p = row + l;
+      double2 acc = make_double2(0.0, 0.0);
+      for (uint32_t x = 0; x < g.nx; x++) { acc.x += p[x * sx].x; acc.y += p[x * sx].y; p[x * sx] = acc; }
+    }
   }
   __syncthreads();
   if (!jv) return;
@@ -704,19 +681,6 @@ __device__ __forceinline__ void shell_block(const Grid &g, const SatArgs &a, uin
   const uint32_t radii = a.node_radii[k];
   const uint32_t r_out = radii >> 16, r_in = radii & 0xffffu;
   const double w = a.node64[k].w;
-  auto shell = [&](uint32_t x, uint32_t y, uint32_t z) {
-    // padded corner coordinates of the outer and inner cube, per axis
-    const uint32_t xo0 = (x > r_out ? x - r_out : 0u) * sx, xo1 = (min(x + r_out, g.nx - 1) + 1) * sx;
-    const uint32_t yo0 = (y > r_out ? y - r_out : 0u) * sy, yo1 = (min(y + r_out, g.ny - 1) + 1) * sy;
-    const uint32_t zo0 = (z > r_out ? z - r_out : 0u), zo1 = min(z + r_out, g.nz - 1) + 1;
-    const uint32_t xi0 = (x > r_in ? x - r_in : 0u) * sx, xi1 = (min(x + r_in, g.nx - 1) + 1) * sx;
-    const uint32_t yi0 = (y > r_in ? y - r_in : 0u) * sy, yi1 = (min(y + r_in, g.ny - 1) + 1) * sy;
-    const uint32_t zi0 = (z > r_in ? z - r_in : 0u), zi1 = min(z + r_in, g.nz - 1) + 1;
-    const double2 o = box_padded(row, xo0, xo1, yo0, yo1, zo0, zo1);
-    const double2 i = box_padded(row, xi0, xi1, yi0, yi1, zi0, zi1);
-    const double2 sh = make_double2((o.x - i.x) * w, (o.y - i.y) * w);
-    return cmul(cmul(sh, twx[x]), cmul(twy[y], twz[z]));
-  };
   // The thread's cells c = first + i * step.  Small grids (several nodes per
   // CTA) look their coordinates up in the CTA's table.  Large grids (one node
   // per CTA) step them with carries: there the table cost every CTA two
@@ -726,21 +690,28 @@ __device__ __forceinline__ void shell_block(const Grid &g, const SatArgs &a, uin
   if constexpr (kMinBlocks > 1) {
     for (uint32_t c = first; c < C; c += step) {
       const uint32_t xyz = a.xyz_table ? s_xyz[c] : coords(c);
-      const double2 r = shell(xyz & 1023u, (xyz >> 10) & 1023u, xyz >> 20);
+      const uint32_t x = xyz & 1023u, y = (xyz >> 10) & 1023u, z = xyz >> 20;
+      const double2 o = cube_sum(row, x, y, z, r_out, g);
+      const double2 i = cube_sum(row, x, y, z, r_in, g);
+      const double2 sh = make_double2((o.x - i.x) * w, (o.y - i.y) * w);
+      const double2 r = cmul(cmul(sh, twx[x]), cmul(twy[y], twz[z]));
       a.R[sr_index(c, ks, C)] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
     }
   } else {
     const uint32_t syz = g.ny * g.nz;
-    const uint32_t dx = step / syz, dy = (step - dx * syz) / g.nz, dz = step - dx * syz - dy * g.nz;
+    const uint32_t sx = step / syz, sy = (step - sx * syz) / g.nz, sz = step - sx * syz - sy * g.nz;
     uint32_t x = first / syz, y = (first - x * syz) / g.nz, z = first - x * syz - y * g.nz;
     for (uint32_t c = first; c < C; c += step) {
-      const double2 r = shell(x, y, z);
+      const double2 o = cube_sum(row, x, y, z, r_out, g);
+      const double2 i = cube_sum(row, x, y, z, r_in, g);
+      const double2 sh = make_double2((o.x - i.x) * w, (o.y - i.y) * w);
+      const double2 r = cmul(cmul(sh, twx[x]), cmul(twy[y], twz[z]));
       a.R[sr_index(c, ks, C)] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
-      z += dz;  // dz < nz and dy < ny: one carry at most per axis
+      z += sz;  // sz < nz and sy < ny: one carry at most per axis
       if (z >= g.nz) { z -= g.nz; y++; }
-      y += dy;
+      y += sy;
       if (y >= g.ny) { y -= g.ny; x++; }
-      x += dx;
+      x += sx;
     }
   }
 }
@@ -948,8 +919,12 @@ constexpr int kLrfSlotPad = 2;
 constexpr int kLrfSlot = kLrfTilePairs + kLrfSlotPad;
 constexpr int kLrfPerThread = (kLrfCells * kLrfTilePairs) / kLrThreads;
 constexpr int kLrGroup = 14;      // node pairs per group (even: radial scales load as quads)
-constexpr int kLrPolyStride = 7;  // pair q of a group is on the FMA pipe when q % 7 == 6
 static_assert(kLrGroup % 2 == 0, "groups are whole radial-scale quads");
+// Which pairs of a group take the FMA-pipe polynomial: bit q of the mask.
+// The variants are compiled in and chosen per plan by the autotuner
+// (glst_autotune); variant 0, two pairs in fourteen, is the default.
+constexpr uint32_t kLrPolyMasks[4] = {(1u << 6) | (1u << 13), 0u, 1u << 13, (1u << 4) | (1u << 9) | (1u << 13)};
+constexpr int kLrVariants = 4;
 
 __device__ __forceinline__ uint32_t cell_of_atom(const uint32_t *__restrict__ cell_point, uint32_t ncell,
                                                  uint32_t p) {
@@ -963,6 +938,7 @@ __device__ __forceinline__ uint32_t cell_of_atom(const uint32_t *__restrict__ ce
   return lo;
 }
 
+template <uint32_t kPolyMask>
 __device__ __forceinline__ void lr_block(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_point,
                                          uint32_t ncell, const LrChunk *__restrict__ chunks,
                                          const float4 *__restrict__ dirs, const float *__restrict__ kappa,
@@ -1040,10 +1016,9 @@ __device__ __forceinline__ void lr_block(const float4 *__restrict__ pk, const ui
           const float2 u2 = bcast(u);
           float2 EA = make_float2(0.f, 0.f), EB = make_float2(0.f, 0.f), G = make_float2(0.f, 0.f);
           const float4 *nn = cb + d * npr;
-          // Groups of kLrGroup pairs: pair q with q % kLrPolyStride ==
-          // kLrPolyStride - 1 takes its sine and cosine from the FMA-pipe
-          // polynomial, interleaved with the SFU pairs of its group; the
-          // remaining pairs use the SFU.  The radial scales of two pairs come
+          // Groups of kLrGroup pairs: pair q with bit q of kPolyMask takes
+          // its sine and cosine from the FMA-pipe polynomial, interleaved
+          // with the SFU pairs of its group; the remaining pairs use the SFU.  The radial scales of two pairs come
           // in one 16-byte load (the R' pair and the scales were two shared
           // loads per node pair in the MIO queue beside four MUFU operations).
           auto sfu_pair = [&](const float4 &v, float2 kp) {
@@ -1065,7 +1040,7 @@ __device__ __forceinline__ void lr_block(const float4 *__restrict__ pk, const ui
               if ((q & 1) == 0) kq = s_kappa4[(k + q) >> 1];
               const float2 kp = (q & 1) ? make_float2(kq.z, kq.w) : make_float2(kq.x, kq.y);
               const float4 v = nn[k + q];
-              if (q % kLrPolyStride == kLrPolyStride - 1) {
+              if ((kPolyMask >> q) & 1u) {
                 const float2 th = __fmul2_rn(kp, u2);
                 float2 C, Sn, sg;
                 fma_sincos_signed2(th, 1.0f, &Sn, &C, &sg);  // sg = (+-1, +-1)
@@ -1116,13 +1091,14 @@ __device__ __forceinline__ void lr_block(const float4 *__restrict__ pk, const ui
   }
 }
 
+template <int kVariant>
 __global__ void __launch_bounds__(kLrThreads, 8)
 k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_point, uint32_t ncell,
                   const LrChunk *__restrict__ chunks, const float4 *__restrict__ dirs,
                   const float *__restrict__ kappa, const float2 *__restrict__ R, uint32_t node_off,
                   uint32_t natom, int accumulate, double4 *__restrict__ part) {
-  lr_block(pk, cell_point, ncell, chunks, dirs, kappa, R, node_off, natom, accumulate, part, blockIdx.x,
-           blockIdx.y);
+  lr_block<kLrPolyMasks[kVariant]>(pk, cell_point, ncell, chunks, dirs, kappa, R, node_off, natom, accumulate,
+                                   part, blockIdx.x, blockIdx.y);
 }
 
 // ----------------------------------------------------------------------------

@@ -113,14 +113,16 @@ __global__ void __launch_bounds__(kSatThreads, 3) k_shell_sums_multi(const SysDe
 }
 
 // item (a, b) = (block of kLrThreads atoms, long-range chunk); seven CTAs per
-// SM, as the structure factors
+// SM, as the structure factors; the default polynomial share (the work
+// list takes only systems with the default launch variants)
 __global__ void __launch_bounds__(kLrThreads, 7) k_long_range_multi(const SysDesc *__restrict__ sys,
                                                                     const WorkItem *__restrict__ items,
                                                                     uint32_t n) {
   for (uint32_t it = blockIdx.x; it < n; it += gridDim.x) {
     const WorkItem w = items[it];
     const SysDesc &d = sys[w.sys];
-    lr_block(d.pk, d.cell_point, d.g.ncell, d.chunks, d.dirs, d.kappa, d.R, 0, d.natom, 0, d.part, w.a, w.b);
+    lr_block<kLrPolyMasks[0]>(d.pk, d.cell_point, d.g.ncell, d.chunks, d.dirs, d.kappa, d.R, 0, d.natom, 0,
+                              d.part, w.a, w.b);
     __syncthreads();
   }
 }

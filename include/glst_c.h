@@ -79,6 +79,12 @@ typedef struct glst_info {
   uint32_t shell_sums_global; /* 1: the grid's per-node prefix table does not
                                fit in shared memory; shell sums build their
                                tables in global memory (any grid size) */
+  uint32_t gather_variant;  /* share of the gather's sines/cosines on the FMA
+                               pipe: 0 = 2 in 14 node pairs (default), 1 =
+                               none, 2 = 1 in 14, 3 = 3 in 14 (glst_autotune) */
+  uint32_t sf_max_npt;      /* radial nodes per thread, at most, in the
+                               structure-factor units (12 by default;
+                               glst_autotune) */
 } glst_info;
 
 /* Where spherical t-designs are read from.  Either the project's binary store
@@ -205,12 +211,15 @@ glst_status glst_plan(uint32_t natom, double tol, double box_x, double box_y,
                       double *kx, double *ky, double *kz, double *w,
                       uint32_t *group);
 
-/* Autotuner: times the shell-sum kernel for 1..32 nodes per CTA and the
- * long-range gather for 2..32 waves of chunk CTAs on these inputs (device
- * FP64 arrays, as glst_compute), keeps the fastest for this handle, and
- * remembers them for every later handle of the same shape (cells, nodes,
- * atom-count bucket) in this process.  Returns the choice.  Waits for the
- * stream; outputs must be recomputed afterwards.  No reference counterpart. */
+/* Autotuner: times, on these inputs (device FP64 arrays, as glst_compute),
+ * the shell-sum kernel for 1..32 nodes per CTA, the long-range gather for
+ * 2..32 waves of chunk CTAs and for each of its compiled FMA-pipe sine/cosine
+ * shares, and the structure factors for 12 / 8 / 6 radial nodes per thread;
+ * keeps the fastest for this handle, and remembers them for every later
+ * handle of the same shape (cells, nodes, atom-count bucket) in this process.
+ * Returns the first two choices (glst_get_info reports the others).  Waits for
+ * the stream; outputs must be recomputed afterwards.  Handles whose far field
+ * runs in one node stage only.  No reference counterpart. */
 glst_status glst_autotune(glst_handle *h, const double *d_rx,
                           const double *d_ry, const double *d_rz,
                           const double *d_qc, void *stream, uint32_t *sat_nb,
