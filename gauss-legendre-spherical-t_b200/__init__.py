@@ -360,10 +360,9 @@ class GlstBatch:
     systems: sequence of dicts with natom, tol, box (3), rcut.  Inputs and
     outputs are concatenated in system order (``offsets`` gives the starts).
     ``compute(..., plain=False)`` runs one captured CUDA graph over all
-    systems (one persistent launch per phase over a work list of every
-    system's blocks, beside the launch sequences of systems that do not fit
-    the work-list kernels); ``plain=True`` solves them one after another
-    (baseline).
+    systems (their launch sequences on parallel branches; ``mode="worklist"``:
+    one launch per phase over a work list of every system's blocks);
+    ``plain=True`` solves them one after another (baseline).
     """
 
     def __init__(self, systems, ct="double", nstreams=16):
@@ -398,13 +397,14 @@ class GlstBatch:
     def __exit__(self, *exc):
         self.close()
 
-    MODES = {"worklist": 0, "plain": 1, "branches": 2}
+    MODES = {"branches": 0, "plain": 1, "worklist": 2}
 
     def compute(self, x, y, z, q, fx, fy, fz, en, plain=False, stream=None, mode=None):
-        """mode: "worklist" (default; one launch per phase for every system
-        that fits the work-list kernels, the others on graph branches),
-        "branches" (every system its own launch sequence, graph branches),
-        "plain" (one system after another; also plain=True)."""
+        """mode: "branches" (default; every system its own launch sequence
+        on parallel branches of one captured graph), "plain" (one system
+        after another; also plain=True), "worklist" (one launch per phase for
+        every system that fits the work-list kernels, the others on
+        branches)."""
         m = self.MODES[mode] if mode is not None else (1 if plain else 0)
         _check(self._lib.glst_batch_compute(self._b, _ptr(x), _ptr(y), _ptr(z), _ptr(q), _ptr(fx), _ptr(fy),
                                             _ptr(fz), _ptr(en), m, _stream(stream)))

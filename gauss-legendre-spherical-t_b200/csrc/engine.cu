@@ -311,6 +311,10 @@ static uint64_t stage_budget() {
   return b;
 }
 
+// Nodes per gather chunk, at most (a CTA's work is 128 atoms x its chunk's
+// nodes; water10k's chunks hold ~1,800 nodes).
+static constexpr size_t kMaxChunkNodes = 2048;
+
 static uint32_t pow2_floor(uint32_t v) {
   uint32_t p = 1;
   while (p * 2 <= v && p < 32) p *= 2;
@@ -400,8 +404,10 @@ static glst_status build_chunks(glst_handle *h, bool in_arena = false) {
     glst_handle::FarRange rg{};
     rg.kb = dirs_all[sd.first].k - kb;
     rg.ke = dirs_all[sd.second - 1].k + dir_nodes(dirs_all[sd.second - 1]) - kb;
-    const size_t target_nodes =
-        std::max<size_t>(1, (h->nshards > 1 ? Kall / nst_sys : rg.ke - rg.kb) / want_chunks);
+    // ... and at most kMaxChunkNodes nodes, so that on large systems (few
+    // chunks fill the GPU) the last wave of gather CTAs stays short
+    const size_t target_nodes = std::max<size_t>(
+        1, std::min<size_t>(kMaxChunkNodes, (h->nshards > 1 ? Kall / nst_sys : rg.ke - rg.kb) / want_chunks));
     rg.c0 = (uint32_t)chunks.size();
     rg.u0 = (uint32_t)units.size();
     size_t i = sd.first;
@@ -1736,16 +1742,17 @@ static glst_status batch_one(glst_batch *b, uint32_t i, const double *const in[4
   return GLST_OK;
 }
 
-// Graph of one batched solve.  mode 0: the work-list systems by one launch
-// per phase on branch 0, every other system its own launch sequence on the
-// remaining branches; mode 2: every system its own launch sequence on the
-// branches (large systems on branch 0, the rest spread over the others).
+// Graph of one batched solve.  mode 0: every system its own launch sequence
+// on the branches (large systems on branch 0, the rest spread over the
+// others); mode 2: the work-list systems by one launch per phase (in groups
+// on the first branches), every other system its own launch sequence on the
+// remaining branches.
 static glst_status batch_capture(glst_batch *b, const double *const in[4], double *const out[4], int mode) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   b->exec = nullptr;
   b->graph = nullptr;
-  const bool wl = mode == 0 && !b->wl.empty();
+  const bool wl = mode == 2 && !b->wl.empty();
   if (wl) GLST_TRY(worklist_descriptors(b, in, out));
   CUDA_TRY(cudaStreamBeginCapture(b->own, cudaStreamCaptureModeThreadLocal));
   glst_status s = GLST_OK;
@@ -1983,11 +1990,14 @@ uint64_t estimate_bytes(const Plan &p, int nsm) {
   uint64_t b = N * (4 * 4 + 16 + 32 + 32 * dev::kSrPlanes + 8 * 8 + 32) + C * 8 + 4096;
   if (K) {
     const uint64_t slots = (uint64_t)nsm * 16;
-    const uint64_t chunks = std::max<uint64_t>(1, (8 * slots + C - 1) / C) + p.groups.size() + 1;
     const uint64_t kpad = (K + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock;
     const uint64_t nst = std::max<uint64_t>(1, (C * kpad * 16 + stage_budget() - 1) / stage_budget());
     // the largest stage: ~K / stages, plus up to one direction's nodes
     const uint64_t stage_k = std::min<uint64_t>(kpad, (K + nst - 1) / nst + 2 * dev::kLrfTileNodes);
+    // gather chunks of a stage (partial rows): enough to fill the GPU, at
+    // most kMaxChunkNodes nodes each, one more per group boundary
+    const uint64_t chunks = std::max<uint64_t>((8 * slots + C - 1) / C, stage_k / kMaxChunkNodes + 1) +
+                            p.groups.size() + 1;
     const uint64_t stage_kpad = (stage_k + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock;
     b += K * (32 + 4 + 16 + 4) + C * stage_kpad * (8 + 8) + chunks * N * 32;
     // global-memory shell-sum tables (grids whose per-node table exceeds the

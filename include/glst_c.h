@@ -286,18 +286,20 @@ glst_status glst_batch_destroy(glst_batch *b);
 
 /* Solve every system.  `plain` selects the schedule:
  *   0: one captured CUDA graph (captured on the first call and again whenever
- *      the pointers or the mode change) in which every system that fits the
- *      work-list kernels (whole system, one node stage, shell sums in shared
- *      memory) is solved by ONE persistent launch per phase -- assignment,
- *      structure factors, shell sums, gather, near field, combine -- over a
- *      work list of (system, unit / cell / node block / atom block x chunk)
- *      items, each item running exactly the code the system's own launch
- *      would; the other systems run their own launch sequences on parallel
- *      graph branches beside it;
+ *      the pointers or the mode change) of every system's own launch
+ *      sequence, spread over `nstreams` parallel branches (systems assigned
+ *      largest first to the least loaded branch, those that fill the GPU
+ *      alone on one branch) -- the fastest schedule measured;
  *   1: the systems one after another on one stream, each its own launch
  *      sequence (the one-system-per-launch baseline);
- *   2: one captured graph of every system's own launch sequence spread over
- *      `nstreams` branches.
+ *   2: one captured graph in which every system that fits the work-list
+ *      kernels (whole system, one node stage, shell sums in shared memory,
+ *      default launch variants) is solved by one launch per phase --
+ *      assignment, structure factors, shell sums, gather, near field,
+ *      combine -- over a work list of (system, unit / cell / node block /
+ *      atom block x chunk) items, each item running exactly the code the
+ *      system's own launch would (in groups on parallel branches); the other
+ *      systems run their own launch sequences beside them.
  * Every mode gives every system bit for bit the result it gets alone.
  * Outputs in input order per system.  Stream ordered. */
 glst_status glst_batch_compute(glst_batch *b, const double *d_rx,

@@ -17,8 +17,8 @@ def _cat(systems, key):
 
 
 def test_batch_equals_individual_solves(pkg):
-    """Ten uneven systems (a few without far field): the work-list graph, its
-    replay, the plain sequence and the branch graph all give every system
+    """Ten uneven systems (a few without far field): the branch graph, its
+    replay, the plain sequence and the work-list graph all give every system
     bit for bit its result alone."""
     from glst_b200 import systems as S
     sy = S.batch_uneven(10, seed=3, mol_min=100, mol_max=2500)
@@ -36,7 +36,7 @@ def test_batch_equals_individual_solves(pkg):
         b.compute(*ins, *outs, plain=True)     # one system after another
         torch.cuda.synchronize()
         plain = [o.cpu().numpy().copy() for o in outs]
-        b.compute(*ins, *outs, mode="branches")  # each system its own launches, graph branches
+        b.compute(*ins, *outs, mode="worklist")  # one launch per phase over the work list
         torch.cuda.synchronize()
         branches = [o.cpu().numpy().copy() for o in outs]
         e_branches = b.energies()
