@@ -500,6 +500,7 @@ def run_ours(args, world, rank, local, dist):
         "data": "synthetic (seeded TIP3P-like water, no dataset)",
         "config": {"workload": args.workload, "atoms": n, "box_A": L, "rcut_A": sysd["rcut"],
                    "tol": sysd["tol"], "cells": list(inf.ncell), "groups": inf.ngroup, "nodes": K,
+                   "node_stages": inf.node_stages, "device_bytes": int(inf.device_bytes),
                    "parallelism": "dp%d (independent systems)" % world,
                    "l2": "flushed (256 MB write) between timed steps"},
         "clocks": clk,
@@ -507,6 +508,9 @@ def run_ours(args, world, rank, local, dist):
                 "path": "glst_compute_host (pinned host buffers, H2D + solve + D2H per step)"},
         "gpu_launches": int(inf.kernels_per_compute) * args.steps,
         "phases_ms": phases,
+        "phases_note": ("phase by phase through the reference's phase methods; with several node stages "
+                        "calc_sf runs the whole staged far field" if inf.node_stages > 1 else
+                        "phase by phase through the reference's phase methods"),
         "roofline": roofline,
         "wall_s_timed": wall,
     }
