@@ -299,11 +299,11 @@ static Tuning tuned(const Plan &p, uint32_t K) {
   return it == g_tune.end() ? Tuning{} : it->second;
 }
 
-// Bytes of S + R one node stage may hold (default 2 GiB; the environment
+// Bytes of S + R one node stage may hold (default 4 GiB; the environment
 // variable GLST_STAGE_BYTES, read when a handle is set up, overrides it).
 // Systems whose C x K operand is larger run in several stages.
 static uint64_t stage_budget() {
-  uint64_t b = 2ull << 30;
+  uint64_t b = 4ull << 30;
   if (const char *e = std::getenv("GLST_STAGE_BYTES")) {
     const unsigned long long x = std::strtoull(e, nullptr, 10);
     if (x >= (1ull << 20)) b = x;
@@ -379,11 +379,19 @@ static glst_status build_chunks(glst_handle *h, bool in_arena = false) {
   nst = std::min<uint64_t>(nst, std::max<size_t>(1, d1 - d0));
   std::vector<std::pair<size_t, size_t>> stage_dirs;  // [first, last) direction of each stage
   {
+    // directions per structure-factor unit of group gi: a stage ends on a
+    // unit boundary of its group (no partial unit inside a group's run but
+    // at its end), or at the end of a group
+    auto dpu = [&](uint32_t gi) {
+      const uint32_t nr = p.groups[gi].n_radial;
+      return (uint32_t)dev::kSfThreads / ((nr + h->sf_max_npt - 1) / h->sf_max_npt);
+    };
     size_t i = d0;
     for (uint64_t st = 0; st < nst && i < d1; st++) {
       const uint64_t target_end = kb + K * (st + 1) / nst;  // node where this stage should end
       size_t e = i + 1;
       while (e < d1 && dirs_all[e].k < target_end) e++;
+      while (e < d1 && dirs_all[e].gi == dirs_all[e - 1].gi && dirs_all[e].j % dpu(dirs_all[e].gi) != 0) e++;
       if (st + 1 == nst) e = d1;
       stage_dirs.push_back({i, e});
       i = e;
@@ -1992,8 +2000,12 @@ uint64_t estimate_bytes(const Plan &p, int nsm) {
     const uint64_t slots = (uint64_t)nsm * 16;
     const uint64_t kpad = (K + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock;
     const uint64_t nst = std::max<uint64_t>(1, (C * kpad * 16 + stage_budget() - 1) / stage_budget());
-    // the largest stage: ~K / stages, plus up to one direction's nodes
-    const uint64_t stage_k = std::min<uint64_t>(kpad, (K + nst - 1) / nst + 2 * dev::kLrfTileNodes);
+    // the largest stage: ~K / stages, plus up to one structure-factor unit of
+    // directions (stages end on unit boundaries)
+    uint32_t max_nr = 1;
+    for (const auto &g : p.groups) max_nr = std::max(max_nr, g.n_radial);
+    const uint64_t stage_k =
+        nst == 1 ? kpad : std::min<uint64_t>(kpad, (K + nst - 1) / nst + (uint64_t)dev::kSfThreads * max_nr);
     // gather chunks of a stage (partial rows): enough to fill the GPU, at
     // most kMaxChunkNodes nodes each, one more per group boundary
     const uint64_t chunks = std::max<uint64_t>((8 * slots + C - 1) / C, stage_k / kMaxChunkNodes + 1) +

@@ -735,7 +735,7 @@ struct GsatArgs {
   const float2 *S;              // stage-local structure factors
   const double4 *node64;        // node table of the stage (kx, ky, kz, w)
   const uint32_t *node_radii;   // r_in | r_out << 16, same indexing
-  const double2 *tw;            // per stage node: nx + ny + nz twiddles e^{+i k_a c_a}
+  const double2 *tw;            // twiddles e^{+i k_a c_a}: tw[a * K + k], a = 0 .. nx + ny + nz - 1
   double2 *T;                   // tables of the batch: nblk x C x kNodeBlock
   float2 *R;                    // stage-local shell sums
   uint32_t K;                   // nodes of the stage
@@ -743,13 +743,15 @@ struct GsatArgs {
   uint32_t nblk;                // node blocks in the batch
 };
 
-// Twiddle table: tw[k * (nx + ny + nz) + a] = e^{+i k_axis (i + 1/2) l}.
+// Twiddle table: tw[a * K + k] = e^{+i k_axis (i + 1/2) l} for the a-th of
+// the nx + ny + nz per-axis cell indices (node fastest, so the warps of the
+// passes, 32 consecutive nodes each, read contiguous runs).
 __global__ void k_gsat_twiddles(Grid g, const double4 *__restrict__ node64, uint32_t K,
                                 double2 *__restrict__ tw) {
   const uint32_t naxis = g.nx + g.ny + g.nz;
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (size_t)K * naxis) return;
-  const uint32_t k = (uint32_t)(t / naxis), r = (uint32_t)(t - (size_t)k * naxis);
+  const uint32_t r = (uint32_t)(t / K), k = (uint32_t)(t - (size_t)r * K);
   const double4 nk = node64[k];
   double kc;
   if (r < g.nx) kc = nk.x * cell_centre(r, g.l);
@@ -774,7 +776,7 @@ __global__ void k_gsat_z(Grid g, GsatArgs a) {
   if (line >= (size_t)g.nx * g.ny) return;
   const uint32_t blk = a.blk0 + bb;
   const uint32_t k = blk * kNodeBlock + j;  // stage-local node
-  const uint32_t C = g.ncell, naxis = g.nx + g.ny + g.nz;
+  const uint32_t C = g.ncell;
   const uint32_t x = (uint32_t)(line / g.ny), y = (uint32_t)(line - (size_t)x * g.ny);
   const uint32_t c0 = (uint32_t)line * g.nz;
   double2 *T = a.T;
@@ -782,14 +784,15 @@ __global__ void k_gsat_z(Grid g, GsatArgs a) {
     for (uint32_t z = 0; z < g.nz; z++) T[gsat_at(bb, c0 + z, j, C)] = make_double2(0.0, 0.0);
     return;
   }
-  const double2 *tk = a.tw + (size_t)k * naxis;
-  const double2 txy = cmul(tk[x], tk[g.nx + y]);
-  const double2 *twz = tk + g.nx + g.ny;
+  const size_t K = a.K;
+  const double2 *tk = a.tw + k;  // entry of axis index i: tk[i * K]
+  const double2 txy = cmul(tk[(size_t)x * K], tk[(size_t)(g.nx + y) * K]);
+  const double2 *twz = tk + (size_t)(g.nx + g.ny) * K;
   double2 acc = make_double2(0.0, 0.0);
 #pragma unroll 4
   for (uint32_t z = 0; z < g.nz; z++) {
     const float2 v = a.S[sr_index(c0 + z, k, C)];
-    const double2 tt = cmul(txy, twz[z]);
+    const double2 tt = cmul(txy, twz[(size_t)z * K]);
     const double vx = v.x, vy = v.y;
     acc.x += vx * tt.x + vy * tt.y;  // v * conj(tt)
     acc.y += vy * tt.x - vx * tt.y;
@@ -865,8 +868,9 @@ __global__ void k_gsat_shell(Grid g, GsatArgs a) {
   const double2 o = gcube_sum(a.T, bb, j, x, y, z, r_out, g);
   const double2 i = gcube_sum(a.T, bb, j, x, y, z, r_in, g);
   const double2 sh = make_double2((o.x - i.x) * w, (o.y - i.y) * w);
-  const double2 *tk = a.tw + (size_t)k * (g.nx + g.ny + g.nz);
-  const double2 r = cmul(cmul(sh, tk[x]), cmul(tk[g.nx + y], tk[g.nx + g.ny + z]));
+  const size_t K = a.K;
+  const double2 *tk = a.tw + k;
+  const double2 r = cmul(cmul(sh, tk[(size_t)x * K]), cmul(tk[(size_t)(g.nx + y) * K], tk[(size_t)(g.nx + g.ny + z) * K]));
   a.R[sr_index((uint32_t)c, k, g.ncell)] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
 }
 
