@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--profile-batch", default=None, choices=["branches", "plain", "worklist"],
+                    help="only create the 256-box batch and solve it twice in this mode (a short process "
+                         "for an ncu launch list of the batch's kernels), then exit")
     ap.add_argument("--reference-log", default=None, metavar="PATH",
                     help="also write the flagship run as a log in the reference driver's layout "
                          "(test/full_example.cu), which utils/parse_glst_results.py reads")
@@ -457,7 +460,7 @@ def run_ours(args, world, rank, local, dist):
         "bound": "sfu", "kernel": dom, "achieved": achieved_sfu / 1e9, "peak": sfu_peak / 1e9,
         "unit": "G sincos-results/s", "frac": achieved_sfu / sfu_peak,
         "peak_source": "measured on this GPU by glst_measure_pipe_peaks (MUFU sin+cos loop)",
-        "traffic": 3.208e8 if dom == "long_range" else 2.196e8,
+        "traffic": 3.197e8 if dom == "long_range" else 2.298e8,
         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of this "
                           "kernel on this workload (profiles/water10k_solve_kernels.md)",
         "pairs_per_launch": pairs,
@@ -533,8 +536,26 @@ def run_ours(args, world, rank, local, dist):
     f.close()
 
 
+def profile_batch(mode):
+    import torch
+    g = __graft_entry__.load_package()
+    from glst_b200 import systems
+    dev = torch.device("cuda", 0)
+    sy = systems.batch_uneven(256, seed=0)
+    ins = [torch.tensor(np.concatenate([s[k] for s in sy]), dtype=torch.float64, device=dev)
+           for k in ("x", "y", "z", "q")]
+    outs = [torch.empty(ins[0].numel(), dtype=torch.float64, device=dev) for _ in range(4)]
+    with g.GlstBatch(sy, nstreams=16) as b:
+        for _ in range(2):
+            b.compute(*ins, *outs, mode=mode)
+        torch.cuda.synchronize()
+
+
 def main():
     args = parse()
+    if args.profile_batch:
+        profile_batch(args.profile_batch)
+        return
     world, rank, local, dist = dist_setup(args)
     try:
         if args.impl == "reference":

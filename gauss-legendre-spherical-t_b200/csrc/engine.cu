@@ -709,7 +709,6 @@ static glst_status phase_assign(glst_handle *h, const double *rx, const double *
   const uint32_t N = h->plan.natom, C = h->plan.ncell;
   if (N && (!rx || !ry || !rz || !qc)) return fail(GLST_ERR_INVALID_ARG, "null input pointer");
   CUDA_TRY(cudaMemsetAsync(h->cell_count, 0, C * sizeof(uint32_t), st));
-  CUDA_TRY(cudaMemsetAsync(h->flags, 0, 4 * sizeof(uint32_t), st));
   if (N) {
     const uint32_t nb = (N + 255) / 256;
     dev::k_bin<<<nb, 256, 0, st>>>(rx, ry, rz, N, h->grid, h->atom_cell, h->atom_slot, h->cell_count);
@@ -859,24 +858,33 @@ static glst_status phase_sr(glst_handle *h, cudaStream_t st) {
   return GLST_OK;
 }
 
-static glst_status phase_combine(glst_handle *h, cudaStream_t st) {
+// Where a solve's input-order outputs and total energy go: the handle's own
+// buffers, or (a batch) slices of the batch's arrays.
+struct OutDest {
+  double *ofx = nullptr, *ofy = nullptr, *ofz = nullptr, *oen = nullptr, *energy = nullptr;
+};
+
+static glst_status phase_combine(glst_handle *h, cudaStream_t st, const OutDest *od = nullptr) {
   const uint32_t N = h->plan.natom;
+  double *ofx = od && od->ofx ? od->ofx : h->ofx, *ofy = od && od->ofy ? od->ofy : h->ofy;
+  double *ofz = od && od->ofz ? od->ofz : h->ofz, *oen = od && od->oen ? od->oen : h->oen;
+  double *energy = od && od->energy ? od->energy : h->energy;
   if (N) {
     dev::k_combine<<<h->combine_blocks, dev::kCombineThreads, 0, st>>>(
         h->sr, h->part, h->part_rows, h->sorted_idx, N, h->K ? 1 : 0, h->cfx, h->cfy, h->cfz, h->cen,
-        h->ofx, h->ofy, h->ofz, h->oen, h->block_energy);
+        ofx, ofy, ofz, oen, h->block_energy);
     CUDA_TRY(cudaGetLastError());
-    dev::k_energy_total<<<1, 256, 0, st>>>(h->block_energy, h->combine_blocks, h->energy);
+    dev::k_energy_total<<<1, 256, 0, st>>>(h->block_energy, h->combine_blocks, energy);
     CUDA_TRY(cudaGetLastError());
   } else {
-    CUDA_TRY(cudaMemsetAsync(h->energy, 0, sizeof(double), st));
+    CUDA_TRY(cudaMemsetAsync(energy, 0, sizeof(double), st));
   }
   h->computed = true;
   return GLST_OK;
 }
 
 static glst_status compute_all(glst_handle *h, const double *rx, const double *ry, const double *rz,
-                               const double *qc, cudaStream_t st) {
+                               const double *qc, cudaStream_t st, const OutDest *od = nullptr) {
   GLST_TRY(phase_assign(h, rx, ry, rz, qc, st));
   // The near field (FP64 pipe) runs on a side stream, overlapping the far
   // field on the same SMs.  It is forked after the (first stage's) structure
@@ -907,7 +915,7 @@ static glst_status compute_all(glst_handle *h, const double *rx, const double *r
   }
   if (!sr_forked) GLST_TRY(fork_sr());
   CUDA_TRY(cudaStreamWaitEvent(st, h->ev_join, 0));
-  return phase_combine(h, st);
+  return phase_combine(h, st, od);
 }
 
 // Entry points run on the handle's device whatever device is current, and
@@ -1737,17 +1745,19 @@ static glst_status worklist_launch(glst_batch *b, glst_batch::WlGroup &gr, cudaS
   return GLST_OK;
 }
 
-// One system: solve, then copy its outputs into the batch's arrays.
+// One system: its solve, the combine writing the input-order outputs and the
+// total energy straight into the batch's arrays (no copies).
 static glst_status batch_one(glst_batch *b, uint32_t i, const double *const in[4], double *const out[4],
                              cudaStream_t st) {
   glst_handle *h = b->sys[i];
-  const size_t o = b->off[i], n = h->plan.natom;
-  GLST_TRY(compute_all(h, in[0] + o, in[1] + o, in[2] + o, in[3] + o, st));
-  double *src[4] = {h->ofx, h->ofy, h->ofz, h->oen};
-  for (int k = 0; k < 4; k++)
-    if (n && out[k]) CUDA_TRY(cudaMemcpyAsync(out[k] + o, src[k], n * sizeof(double), cudaMemcpyDeviceToDevice, st));
-  CUDA_TRY(cudaMemcpyAsync(b->energies + i, h->energy, sizeof(double), cudaMemcpyDeviceToDevice, st));
-  return GLST_OK;
+  const size_t o = b->off[i];
+  OutDest od;
+  od.ofx = out[0] ? out[0] + o : nullptr;
+  od.ofy = out[1] ? out[1] + o : nullptr;
+  od.ofz = out[2] ? out[2] + o : nullptr;
+  od.oen = out[3] ? out[3] + o : nullptr;
+  od.energy = b->energies + i;
+  return compute_all(h, in[0] + o, in[1] + o, in[2] + o, in[3] + o, st, &od);
 }
 
 // Graph of one batched solve.  mode 0: every system its own launch sequence

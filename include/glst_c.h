@@ -311,7 +311,10 @@ glst_status glst_batch_compute(glst_batch *b, const double *d_rx,
 /* Total energy of every system (nsys doubles, host), waits for the stream. */
 glst_status glst_batch_energies(glst_batch *b, double *e, void *stream);
 
-/* Handle of system i (owned by the batch; do not destroy). */
+/* Handle of system i (owned by the batch; do not destroy): its plan
+ * (glst_get_info) and cell-ordered outputs.  A batched solve writes the
+ * input-order outputs and the total energy straight into the batch's arrays
+ * (glst_batch_compute's outputs, glst_batch_energies), not into the handle. */
 glst_status glst_batch_system(glst_batch *b, uint32_t i, glst_handle **h);
 
 /* ---------------------------------------------------------------------------
