@@ -52,7 +52,7 @@ class GlstInfo(ctypes.Structure):
         ("device_bytes", ctypes.c_uint64),
         ("kernels_per_compute", ctypes.c_uint32),
         ("node_stages", ctypes.c_uint32),
-        ("shell_sums_global", ctypes.c_uint32),
+        ("shell_sums_form", ctypes.c_uint32),
         ("gather_variant", ctypes.c_uint32),
         ("sf_max_npt", ctypes.c_uint32),
     ]

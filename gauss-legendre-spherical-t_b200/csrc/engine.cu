@@ -165,6 +165,7 @@ struct glst_handle {
   // streams/events for the near-field fork and the far-field pipeline
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_done = nullptr;  // end of a compute, for glst_reduce_shards
   // Node stages: the far field runs stage by stage (structure factors, shell
   // sums, gather over a contiguous range of whole directions), so S and R
   // hold one stage's nodes; a large system needs a fraction of the C x K
@@ -273,8 +274,9 @@ static void release(glst_handle *h, bool device_idle = false) {
   if (h->side) cudaStreamDestroy(h->side);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
   if (h->ev_join) cudaEventDestroy(h->ev_join);
+  if (h->ev_done) cudaEventDestroy(h->ev_done);
   h->side = nullptr;
-  h->ev_fork = h->ev_join = nullptr;
+  h->ev_fork = h->ev_join = h->ev_done = nullptr;
 }
 
 // ---------------------------------------------------------------- tuning
@@ -554,6 +556,7 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
   CUDA_TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
   CUDA_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&h->ev_done, cudaEventDisableTiming));
   try {
     auto store = get_store();
     h->plan = glst::make_plan(natom, tol, box, rcut, ct_float, *store);
@@ -1164,7 +1167,7 @@ glst_status glst_get_info(const glst_handle *h, glst_info *info) {
     }
   info->kernels_per_compute = h->plan.natom ? 4u + (h->shard == 0 ? 1u : 0u) + far + 2u : 2u;
   info->node_stages = (uint32_t)h->ranges.size();
-  info->shell_sums_global = h->gsat ? 1u : 0u;
+  info->shell_sums_form = h->gsat ? 1u : 0u;
   info->gather_variant = h->lr_variant;
   info->sf_max_npt = h->sf_max_npt;
   return GLST_OK;
@@ -1373,10 +1376,10 @@ glst_status glst_reduce_shards(glst_handle *const *shards, uint32_t n, void *con
       else if (e != cudaSuccess) return fail(GLST_ERR_CUDA, "peer access: %s", cudaGetErrorString(e));
       CUDA_TRY(cudaSetDevice(h->device));
     }
-    // ev_join of shard s: recorded on its own compute stream, on its device
-    CUDA_TRY(cudaEventRecord(h->ev_join, S_(streams[s])));
+    // the shard's own event, recorded on its compute stream, on its device
+    CUDA_TRY(cudaEventRecord(h->ev_done, S_(streams[s])));
     if (h->device != h0->device) CUDA_TRY(cudaSetDevice(h0->device));
-    CUDA_TRY(cudaStreamWaitEvent(st0, h->ev_join, 0));
+    CUDA_TRY(cudaStreamWaitEvent(st0, h->ev_done, 0));
   }
   if (!N) return GLST_OK;
   dev::ShardSet ss{};
@@ -1430,11 +1433,11 @@ glst_status glst_get_far_field(glst_handle *h, double *sf_re, double *sf_im, dou
   for (const auto &rg : h->ranges) {
     const size_t nk = rg.ke - rg.kb;
     const size_t nel = C * ((nk + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock);
-    GLST_TRY(sf_stage(h, rg, st));
-    GLST_TRY(shell_stage(h, rg, st));
     hs.resize(nel);
     hr.resize(nel);
+    GLST_TRY(sf_stage(h, rg, st));
     CUDA_TRY(cudaMemcpyAsync(hs.data(), h->S, nel * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    GLST_TRY(shell_stage(h, rg, st));
     CUDA_TRY(cudaMemcpyAsync(hr.data(), h->R, nel * sizeof(float2), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     for (size_t kl = 0; kl < nk; kl++) {

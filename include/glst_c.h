@@ -76,9 +76,10 @@ typedef struct glst_info {
                                structure factors and shell sums of a stage's
                                nodes are held at a time (large systems hold a
                                fraction of the ncell x K operand) */
-  uint32_t shell_sums_global; /* 1: the grid's per-node prefix table does not
-                               fit in shared memory; shell sums build their
-                               tables in global memory (any grid size) */
+  uint32_t shell_sums_form; /* 0: prefix tables in shared memory, one or more
+                               nodes per CTA; 1: the grid's per-node table
+                               does not fit in shared memory, tables in global
+                               memory (any grid size) */
   uint32_t gather_variant;  /* share of the gather's sines/cosines on the FMA
                                pipe: 0 = 2 in 14 node pairs (default), 1 =
                                none, 2 = 1 in 14, 3 = 3 in 14 (glst_autotune) */

@@ -97,7 +97,7 @@ def test_structure_factors_and_shell_sums_per_phase(pkg, store, shell):
     x, y, z, q, tol, box, rcut = _w1000()
     with _env(GLST_GLOBAL_SHELL_SUMS="1" if shell == "global" else "0"):
         f, _ = _solve(pkg, x, y, z, q, tol, box, rcut)
-    assert f.info().shell_sums_global == (1 if shell == "global" else 0)
+    assert f.info().shell_sums_form == {"shared": 0, "global": 1}[shell]
     p = planner.make_plan(len(x), tol, box, rcut, store)
     assert f.info().ncell_total == 64 and f.info().num_nodes == p.K
     sf, rmt = f.far_field()
@@ -112,6 +112,7 @@ def test_global_shell_sums_match_oracle_end_to_end(pkg, store):
     x, y, z, q, tol, box, rcut = _w1000()
     with _env(GLST_GLOBAL_SHELL_SUMS="1"):
         f, got = _solve(pkg, x, y, z, q, tol, box, rcut)
+    assert f.info().shell_sums_form == 1
     p = planner.make_plan(len(x), tol, box, rcut, store)
     _check(f, got, oracle.glst(x, y, z, q, p), x, y, z, p)
     f.close()
@@ -179,7 +180,7 @@ def test_large_grid_26_cubed(pkg, store):
     box, tol, rcut = (260.0, 260.0, 260.0), 1e-3, 10.0
     f, got = _solve(pkg, x, y, z, q, tol, box, rcut)
     inf = f.info()
-    assert tuple(inf.ncell) == (26, 26, 26) and inf.shell_sums_global == 1
+    assert tuple(inf.ncell) == (26, 26, 26) and inf.shell_sums_form == 1
     p = planner.make_plan(len(x), tol, box, rcut, store)
     rep = _check(f, got, _oracle_chunked(x, y, z, q, p), x, y, z, p)
     print("26^3", rep, "K", p.K)
