@@ -916,6 +916,11 @@ struct LrChunk {
 // The cell slots of a tile are kLrfSlotPad float4 apart beyond the tile so
 // that the up to four addresses a warp reads fall in different shared-memory
 // banks (32.9 M bank conflicts per launch without the pad, 0.25 M with).
+// Two adjacent atoms per thread (256 atoms per CTA, one R' load serving both
+// when they share a cell: 0.75 shared loads per (atom, node pair) instead of
+// 1.5) gave bitwise-equal results but ran 14 % slower (water10k 1.67 vs
+// 1.465 ms; 96 registers, 5 CTAs per SM): the MUFU latency the 32 resident
+// warps hide outweighs the MIO-queue relief.
 constexpr int kLrfCells = 4;           // cells staged per pass
 constexpr int kLrfTilePairs = 128;     // node pairs per cell tile
 constexpr int kLrfTileNodes = 2 * kLrfTilePairs;
