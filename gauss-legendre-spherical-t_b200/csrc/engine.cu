@@ -120,6 +120,7 @@ struct glst_handle {
   size_t sat_per_node = 0;          // shell-sum shared bytes per node
   size_t sat_budget = 0;            // shell-sum shared bytes per CTA, at most
   int nsm = 148;
+  size_t smem_sm = 0;  // shared memory per SM, less four CTAs' system reserve
   std::vector<uint32_t> g_node_base, g_dir_base, g_kappa_base;  // per group, internal order
   uint32_t sat_nb = 1, sat_stride = 0;
   bool sat_xyz = true;  // shell-sum cell-coordinate table in shared memory
@@ -534,6 +535,8 @@ static glst_status set_kernel_attributes(int device, size_t shell_smem) {
   if (shell_smem && !(d & 2)) {
     CUDA_TRY(cudaFuncSetAttribute(dev::k_shell_sums<dev::kSatThreads, 3>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shell_smem));
+    CUDA_TRY(cudaFuncSetAttribute(dev::k_shell_sums<dev::kSatThreadsSmall, 4>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shell_smem));
     CUDA_TRY(cudaFuncSetAttribute(dev::k_shell_sums<dev::kSatThreadsOne, 1>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shell_smem));
     d |= 2;
@@ -636,6 +639,10 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
     int smem_optin = 0, nsm = 148;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
     CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+    int smem_sm = 0, smem_reserved = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, h->device));
+    CUDA_TRY(cudaDeviceGetAttribute(&smem_reserved, cudaDevAttrReservedSharedMemoryPerBlock, h->device));
+    h->smem_sm = (size_t)std::max(0, smem_sm - 4 * smem_reserved);
     // row stride = 1 (mod 8) complex doubles: rows of consecutive nodes start
     // 16 bytes apart modulo 128, so the node-fastest accesses of the shell
     // pass spread over all shared-memory banks
@@ -781,10 +788,13 @@ static glst_status shell_stage(glst_handle *h, const glst_handle::FarRange &rg, 
   dev::SatArgs a{h->S, n64, radii, ke - kb, 0, h->sat_nb, lg, table ? 1u : 0u, h->sat_stride, h->R};
   const uint32_t nblk = (ke - kb + h->sat_nb - 1) / h->sat_nb;
   const size_t smem = h->sat_per_node * h->sat_nb + (table ? (((size_t)h->plan.ncell * 4 + 15) & ~size_t(15)) : 0);
-  // several nodes per CTA: 512 threads, 3 CTAs per SM; one node per CTA
-  // (large grids, one CTA fills the shared memory): 1024 threads
+  // several nodes per CTA: 256 threads, 4 CTAs per SM where four CTAs'
+  // tables fit in shared memory, else 512 threads, 3 CTAs per SM; one node
+  // per CTA (large grids, one CTA fills the shared memory): 1024 threads
   if (h->sat_nb == 1)
     dev::k_shell_sums<dev::kSatThreadsOne, 1><<<nblk, dev::kSatThreadsOne, smem, st>>>(h->grid, a);
+  else if (4 * smem <= h->smem_sm)
+    dev::k_shell_sums<dev::kSatThreadsSmall, 4><<<nblk, dev::kSatThreadsSmall, smem, st>>>(h->grid, a);
   else
     dev::k_shell_sums<dev::kSatThreads, 3><<<nblk, dev::kSatThreads, smem, st>>>(h->grid, a);
   CUDA_TRY(cudaGetLastError());

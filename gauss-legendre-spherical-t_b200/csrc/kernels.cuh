@@ -521,9 +521,21 @@ k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ 
 // eight corners of every box, 0.45 ms skipping the zero-plane corners,
 // against 0.42 ms here -- the larger rows and their zeroing cost more than
 // the index arithmetic saved.)
+// Launch shapes: 512 threads, 3 CTAs per SM; 256 threads, 4 CTAs per SM
+// where four CTAs' tables fit in shared memory (water10k, 8 nodes per CTA:
+// 0.382 against 0.416 ms -- fewer threads per node give each thread more
+// cells over which to spread its set-up, and four CTAs overlap their
+// barrier-separated phases better; 4 nodes per CTA at any shape measured
+// 0.55-0.66 ms); one node per CTA, 1024 threads, on large grids.
 constexpr int kSatThreads = 512;
+constexpr int kSatThreadsSmall = 256;
 constexpr int kSatThreadsOne = 1024;  // one node per CTA (large grids): more warps per SM
-constexpr int kSatLoadBatch = 4;
+// S loads in flight per thread: 8 in the 256-thread form (a 7-cell line in
+// one batch), 4 where the register budget is 40 (8 spilled there)
+template <int kMinBlocks>
+struct SatLoadBatch {
+  static constexpr int value = kMinBlocks == 4 ? 8 : 4;
+};
 
 struct SatArgs {
   const float2 *S;               // cell-relative structure factors
@@ -591,19 +603,20 @@ __device__ __forceinline__ void shell_block(const Grid &g, const SatArgs &a, uin
   const uint32_t ks = a.kbase + k;   // node within S and R
   const bool jv = k < a.K;
   // The S loads run as a flat sequence of batches (line l, z from z0) of
-  // kSatLoadBatch cells each; the first is issued before the twiddle tables,
+  // kLoadBatch cells each; the first is issued before the twiddle tables,
   // whose node loads and FP64 sincos it overlaps (water10k shell sums 0.441
   // vs 0.450 ms; one batch in flight ahead of the one summed, 0.462 ms at a
   // batch of 2 and spilling at 4).
+  constexpr int kLoadBatch = SatLoadBatch<kMinBlocks>::value;
   const uint32_t nlines = g.nx * g.ny;
   const double2 zero = make_double2(0.0, 0.0);
   auto fetch = [&](float2 *dst, uint32_t line, uint32_t zb) {
 #pragma unroll
-    for (int u = 0; u < kSatLoadBatch; u++)
+    for (int u = 0; u < kLoadBatch; u++)
       dst[u] = (jv && line < nlines && zb + u < g.nz) ? __ldg(a.S + sr_index(line * g.nz + zb + u, ks, C))
                                                       : make_float2(0.f, 0.f);
   };
-  float2 v[kSatLoadBatch];
+  float2 v[kLoadBatch];
   uint32_t l = first, z0 = 0;
   fetch(v, l, z0);
   // twiddle tables: e^{i k_a (i + 1/2) l} per node and axis
@@ -634,7 +647,7 @@ __device__ __forceinline__ void shell_block(const Grid &g, const SatArgs &a, uin
   {
     double2 acc = zero, txy = zero;
     while (l < nlines) {
-      uint32_t ln = l, zn = z0 + kSatLoadBatch;
+      uint32_t ln = l, zn = z0 + kLoadBatch;
       if (zn >= g.nz) { ln = l + step; zn = 0; }
       if (z0 == 0) {
         const uint32_t lx = l / g.ny;
@@ -643,7 +656,7 @@ __device__ __forceinline__ void shell_block(const Grid &g, const SatArgs &a, uin
       }
       const uint32_t base = l * g.nz;
 #pragma unroll
-      for (int u = 0; u < kSatLoadBatch; u++) {
+      for (int u = 0; u < kLoadBatch; u++) {
         if (z0 + u < g.nz) {
           const double2 t = cmul(txy, twz[z0 + u]);  // e^{+ik.c}
           const double vx = v[u].x, vy = v[u].y;
