@@ -520,7 +520,10 @@ k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ 
 // need no clipping tests, measured slower on water10k: 0.50 ms loading all
 // eight corners of every box, 0.45 ms skipping the zero-plane corners,
 // against 0.42 ms here -- the larger rows and their zeroing cost more than
-// the index arithmetic saved.)
+// the index arithmetic saved.  Per-node tables of per-axis corner offsets,
+// three shared loads per cell in place of the clipping arithmetic, measured
+// slower too: 0.412 against 0.381 ms, a dependent shared load more per cell
+// in a latency-bound loop.)
 // Launch shapes: 512 threads, 3 CTAs per SM; 256 threads, 4 CTAs per SM
 // where four CTAs' tables fit in shared memory (water10k, 8 nodes per CTA:
 // 0.382 against 0.416 ms -- fewer threads per node give each thread more
