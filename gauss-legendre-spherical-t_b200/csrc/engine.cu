@@ -790,7 +790,7 @@ static glst_status shell_stage(glst_handle *h, const glst_handle::FarRange &rg, 
   const size_t smem = h->sat_per_node * h->sat_nb + (table ? (((size_t)h->plan.ncell * 4 + 15) & ~size_t(15)) : 0);
   // several nodes per CTA: 256 threads, 4 CTAs per SM where four CTAs'
   // tables fit in shared memory, else 512 threads, 3 CTAs per SM; one node
-  // per CTA (large grids, one CTA fills the shared memory): 1024 threads
+  // per CTA (large grids, one CTA fills the shared memory): 512 threads
   if (h->sat_nb == 1)
     dev::k_shell_sums<dev::kSatThreadsOne, 1><<<nblk, dev::kSatThreadsOne, smem, st>>>(h->grid, a);
   else if (4 * smem <= h->smem_sm)

@@ -529,15 +529,20 @@ k_structure_factors(const float4 *__restrict__ pk, const uint32_t *__restrict__ 
 // 0.382 against 0.416 ms -- fewer threads per node give each thread more
 // cells over which to spread its set-up, and four CTAs overlap their
 // barrier-separated phases better; 4 nodes per CTA at any shape measured
-// 0.55-0.66 ms); one node per CTA, 1024 threads, on large grids.
+// 0.55-0.66 ms); one node per CTA, 512 threads, on large grids (22^3 grid:
+// 0.393 ms per 1,534 nodes against 0.399 with 1024 and 0.396 with 768
+// threads; there the node's S loads and R stores, 8 bytes at a 256-byte
+// stride in the node-block layout, take 25 % and 20 % of the time, the
+// corners 19 %, the prefix passes 9 %).
 constexpr int kSatThreads = 512;
 constexpr int kSatThreadsSmall = 256;
-constexpr int kSatThreadsOne = 1024;  // one node per CTA (large grids): more warps per SM
-// S loads in flight per thread: 8 in the 256-thread form (a 7-cell line in
-// one batch), 4 where the register budget is 40 (8 spilled there)
+constexpr int kSatThreadsOne = 512;  // one node per CTA (large grids)
+// S loads in flight per thread: 8 (a 7-cell line in one batch on water10k),
+// 4 in the 512-thread several-nodes form, whose register budget is 40 (8
+// spilled there)
 template <int kMinBlocks>
 struct SatLoadBatch {
-  static constexpr int value = kMinBlocks == 4 ? 8 : 4;
+  static constexpr int value = kMinBlocks == 3 ? 4 : 8;
 };
 
 struct SatArgs {
