@@ -315,8 +315,13 @@ static uint64_t stage_budget() {
 }
 
 // Nodes per gather chunk, at most (a CTA's work is 128 atoms x its chunk's
-// nodes; water10k's chunks hold ~1,800 nodes).
+// nodes; water10k's chunks hold ~1,800 nodes) and at least: every chunk
+// writes a partial row of 32 bytes per atom that the combine reads back, so
+// 256 nodes or more keep that traffic at <= 0.25 byte per (atom, node) pair
+// (the 3,000-atom, 4^3-cell system had 33-node chunks: 28 MB of partial
+// rows, 2 bytes per pair, against 10 MB of S and R).
 static constexpr size_t kMaxChunkNodes = 2048;
+static constexpr size_t kMinChunkNodes = 256;
 
 static uint32_t pow2_floor(uint32_t v) {
   uint32_t p = 1;
@@ -347,12 +352,21 @@ static glst_status build_chunks(glst_handle *h, bool in_arena = false) {
     for (uint32_t j = 0; j < p.groups[gi].n_dir; j++)
       dirs_all.push_back({(uint32_t)gi, j, h->g_node_base[gi] + j * p.groups[gi].n_radial});
   auto dir_nodes = [&](const Dir &d) { return p.groups[d.gi].n_radial; };
+  // The whole system's stage count and chunk size.  A shard cuts its chunks
+  // at the whole system's chunk size, so that its chunks are exactly the
+  // whole system's chunks of its node range (the shards' sum then groups
+  // every FP32 partial sum as the unsharded solve).
+  const uint64_t kpad_sys = (Kall + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock;
+  const uint64_t nst_sys = std::max<uint64_t>(1, (C * kpad_sys * 16 + stage_budget() - 1) / stage_budget());
+  auto chunk_nodes = [&](size_t stage_nodes) {
+    return std::max<size_t>(kMinChunkNodes, std::min<size_t>(kMaxChunkNodes, stage_nodes / want_chunks));
+  };
   // this handle's directions [d0, d1)
   size_t d0 = 0, d1 = dirs_all.size();
   if (h->nshards > 1 && Kall) {
-    // shard by provisional chunks of ~K / want_chunks nodes, each assigned to
-    // the shard its middle node falls in
-    const size_t target = std::max<size_t>(1, Kall / want_chunks);
+    // shard by provisional chunks of the whole system's chunk size, each
+    // assigned to the shard its middle node falls in
+    const size_t target = chunk_nodes(Kall / nst_sys);
     bool any = false;
     size_t i = 0;
     while (i < dirs_all.size()) {
@@ -406,19 +420,14 @@ static glst_status build_chunks(glst_handle *h, bool in_arena = false) {
   h->ranges.clear();
   h->stage_kmax = 0;
   h->part_rows = 1;
-  // A shard cuts its chunks at the whole system's chunk size, so that its
-  // chunks are exactly the whole system's chunks of its node range (the
-  // shards' sum then groups every FP32 partial sum as the unsharded solve).
-  const uint64_t kpad_sys = (Kall + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock;
-  const uint64_t nst_sys = std::max<uint64_t>(1, (C * kpad_sys * 16 + stage_budget() - 1) / stage_budget());
   for (const auto &sd : stage_dirs) {
     glst_handle::FarRange rg{};
     rg.kb = dirs_all[sd.first].k - kb;
     rg.ke = dirs_all[sd.second - 1].k + dir_nodes(dirs_all[sd.second - 1]) - kb;
     // ... and at most kMaxChunkNodes nodes, so that on large systems (few
-    // chunks fill the GPU) the last wave of gather CTAs stays short
-    const size_t target_nodes = std::max<size_t>(
-        1, std::min<size_t>(kMaxChunkNodes, (h->nshards > 1 ? Kall / nst_sys : rg.ke - rg.kb) / want_chunks));
+    // chunks fill the GPU) the last wave of gather CTAs stays short; at least
+    // kMinChunkNodes (partial-row traffic on small systems)
+    const size_t target_nodes = chunk_nodes(h->nshards > 1 ? Kall / nst_sys : rg.ke - rg.kb);
     rg.c0 = (uint32_t)chunks.size();
     rg.u0 = (uint32_t)units.size();
     size_t i = sd.first;
