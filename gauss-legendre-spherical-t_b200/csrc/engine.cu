@@ -120,6 +120,7 @@ struct glst_handle {
   size_t sat_per_node = 0;          // shell-sum shared bytes per node
   size_t sat_budget = 0;            // shell-sum shared bytes per CTA, at most
   int nsm = 148;
+  uint32_t sr_rows = dev::kSrRowsPlanes;  // near-field partial-sum rows
   size_t smem_sm = 0;  // shared memory per SM, less four CTAs' system reserve
   std::vector<uint32_t> g_node_base, g_dir_base, g_kappa_base;  // per group, internal order
   uint32_t sat_nb = 1, sat_stride = 0;
@@ -322,6 +323,12 @@ static uint64_t stage_budget() {
 // rows, 2 bytes per pair, against 10 MB of S and R).
 static constexpr size_t kMaxChunkNodes = 2048;
 static constexpr size_t kMinChunkNodes = 256;
+
+// Near-field rows (kernels.cuh): nine when three rows' CTAs (one per cell
+// and x plane) would be fewer than four per SM.
+static uint32_t sr_rows_for(size_t ncell, int nsm) {
+  return 3 * ncell < 4 * (size_t)std::max(1, nsm) ? dev::kSrRowsLines : dev::kSrRowsPlanes;
+}
 
 static uint32_t pow2_floor(uint32_t v) {
   uint32_t p = 1;
@@ -565,6 +572,7 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
     return fail(GLST_ERR_NO_DEVICE, "no CUDA capable device found");
   }
   CUDA_TRY(cudaGetDevice(&h->device));
+  CUDA_TRY(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device));
   CUDA_TRY(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
   CUDA_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
@@ -632,7 +640,8 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
   GLST_TRY(dalloc_n(h, &h->flags, 4));
   GLST_TRY(dalloc_n(h, &h->pk, N));
   GLST_TRY(dalloc_n(h, &h->pd, N));
-  GLST_TRY(dalloc_n(h, &h->sr, (size_t)dev::kSrPlanes * N));
+  h->sr_rows = sr_rows_for(C, h->nsm);
+  GLST_TRY(dalloc_n(h, &h->sr, (size_t)h->sr_rows * N));
   for (double **o : {&h->cfx, &h->cfy, &h->cfz, &h->cen, &h->ofx, &h->ofy, &h->ofz, &h->oen})
     GLST_TRY(dalloc_n(h, o, N));
   h->combine_blocks = (uint32_t)std::max<size_t>(1, (N + dev::kCombineAtoms - 1) / dev::kCombineAtoms);
@@ -711,7 +720,7 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
     CUDA_TRY(cudaMemcpyAsync(h->dirs, dirs.data(), dirs.size() * sizeof(float4), cudaMemcpyHostToDevice, h->side));
     CUDA_TRY(cudaMemcpyAsync(h->kappa, kap.data(), kap.size() * sizeof(float), cudaMemcpyHostToDevice, h->side));
   }
-  if (shard > 0) CUDA_TRY(cudaMemsetAsync(h->sr, 0, (size_t)dev::kSrPlanes * N * sizeof(double4), h->side));
+  if (shard > 0) CUDA_TRY(cudaMemsetAsync(h->sr, 0, (size_t)h->sr_rows * N * sizeof(double4), h->side));
   GLST_TRY(set_kernel_attributes(h->device, 0));
   CUDA_TRY(cudaMemsetAsync(h->flags, 0, 4 * sizeof(uint32_t), h->side));
   CUDA_TRY(cudaStreamSynchronize(h->side));  // memory and tables ready for any stream
@@ -873,9 +882,9 @@ static glst_status phase_lr(glst_handle *h, cudaStream_t st) {
 
 static glst_status phase_sr(glst_handle *h, cudaStream_t st) {
   if (!h->plan.natom || h->shard > 0) return GLST_OK;  // shard 0 owns the near field
-  dim3 grid(h->plan.ncell, dev::kSrPlanes);
+  dim3 grid(h->plan.ncell, h->sr_rows);
   dev::k_short_range<<<grid, dev::kSrThreads, 0, st>>>(h->pd, h->cell_count, h->cell_point, h->grid,
-                                                       h->plan.natom, h->sr);
+                                                       h->plan.natom, h->sr, h->sr_rows);
   CUDA_TRY(cudaGetLastError());
   return GLST_OK;
 }
@@ -893,7 +902,7 @@ static glst_status phase_combine(glst_handle *h, cudaStream_t st, const OutDest 
   double *energy = od && od->energy ? od->energy : h->energy;
   if (N) {
     dev::k_combine<<<h->combine_blocks, dev::kCombineThreads, 0, st>>>(
-        h->sr, h->part, h->part_rows, h->sorted_idx, N, h->K ? 1 : 0, h->cfx, h->cfy, h->cfz, h->cen,
+        h->sr, h->sr_rows, h->part, h->part_rows, h->sorted_idx, N, h->K ? 1 : 0, h->cfx, h->cfy, h->cfz, h->cen,
         ofx, ofy, ofz, oen, h->block_energy);
     CUDA_TRY(cudaGetLastError());
     dev::k_energy_total<<<1, 256, 0, st>>>(h->block_energy, h->combine_blocks, energy);
@@ -1648,7 +1657,7 @@ static glst_status worklist_build(glst_batch *b, const std::vector<double> &cost
     });
     each(glst_batch::kSr, [&](uint32_t w, glst_handle *h) {
       if (!h->plan.natom) return;
-      for (uint32_t pl = 0; pl < (uint32_t)dev::kSrPlanes; pl++)
+      for (uint32_t pl = 0; pl < h->sr_rows; pl++)
         for (uint32_t c = 0; c < h->plan.ncell; c++) items.push_back({w, c, pl, 0});
     });
     each(glst_batch::kCombine, [&](uint32_t w, glst_handle *h) {
@@ -1723,7 +1732,7 @@ static glst_status worklist_descriptors(glst_batch *b, const double *const in[4]
     d.sorted_idx = h->sorted_idx; d.cell_count = h->cell_count; d.cell_point = h->cell_point;
     d.pk = h->pk; d.pd = h->pd; d.dirs = h->dirs; d.kappa = h->kappa;
     d.chunks = h->chunks; d.sf_units = h->sf_units;
-    d.S = h->S; d.R = h->R; d.part = h->part; d.sr = h->sr;
+    d.S = h->S; d.R = h->R; d.part = h->part; d.sr = h->sr; d.sr_rows = h->sr_rows;
     d.cfx = h->cfx; d.cfy = h->cfy; d.cfz = h->cfz; d.cen = h->cen;
     // input-order outputs straight into the batch's arrays (or the
     // handle's own when the caller passes none)
@@ -2027,7 +2036,7 @@ struct SrvSlot {
 // Device bytes a handle for `p` will hold (an upper bound of setup's sizes).
 uint64_t estimate_bytes(const Plan &p, int nsm) {
   const uint64_t N = p.natom, C = p.ncell, K = p.has_far ? p.K() : 0;
-  uint64_t b = N * (4 * 4 + 16 + 32 + 32 * dev::kSrPlanes + 8 * 8 + 32) + C * 8 + 4096;
+  uint64_t b = N * (4 * 4 + 16 + 32 + 32 * (uint64_t)sr_rows_for(C, nsm) + 8 * 8 + 32) + C * 8 + 4096;
   if (K) {
     const uint64_t slots = (uint64_t)nsm * 16;
     const uint64_t kpad = (K + dev::kNodeBlock - 1) / dev::kNodeBlock * dev::kNodeBlock;

@@ -1140,30 +1140,44 @@ k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ ce
 // fit in the registers the shell-sum blocks leave free) measured slower on
 // water10k: 3.132 / 3.136 ms per solve against 3.122 ms.
 constexpr int kSrThreads = 128;
-constexpr int kSrPlanes = 3;
+// One CTA per (cell, row of neighbour cells) writes one row of per-atom
+// partial sums: 3 rows (the x planes, 9 cells each) or 9 rows (x, y lines,
+// 3 cells each).  Rows are numbered in x-major order of the 27 neighbours;
+// the row holding the cell itself starts with it.  Nine rows shorten each
+// thread's serial run of pairs threefold and triple the CTAs, for grids too
+// small to fill the GPU with three (3,000 atoms on 4^3 cells: 0.076 ->
+// 0.033 ms; 9,000 atoms on 5^3: 0.162 -> 0.092 ms); water10k's 7^3 grid
+// already has 1,029 CTAs, and there nine rows measured 0.2 % slower per
+// solve beside the far field.
+constexpr int kSrRowsPlanes = 3;
+constexpr int kSrRowsLines = 9;
+constexpr int kSrRowsMax = kSrRowsLines;
 
 __device__ __forceinline__ void sr_block(const double4 *__restrict__ pd, const uint32_t *__restrict__ cell_count,
                                          const uint32_t *__restrict__ cell_point, const Grid &g, uint32_t natom,
-                                         double4 *__restrict__ sr, uint32_t cell, uint32_t by) {
+                                         double4 *__restrict__ sr, uint32_t rows, uint32_t cell, uint32_t by) {
   __shared__ double4 s_at[kSrThreads];
-  const int plane = static_cast<int>(by) - 1;  // dx of the neighbour plane
+  const int n = 27 / static_cast<int>(rows);  // neighbour cells per row
+  const int t0 = static_cast<int>(by) * n;    // x-major index of the row's first neighbour
+  const int dx = t0 / 9 - 1;                  // constant along a row
+  const bool own_row = static_cast<int>(by) == 13 / n;
   const uint32_t cnt = cell_count[cell];
   const uint32_t start = cell_point[cell];
   const int ix = cell / (g.ny * g.nz), iy = (cell / g.nz) % g.ny, iz = cell % g.nz;
-  const int jx = ix + plane;
+  const int jx = ix + dx;
   const bool plane_in = jx >= 0 && jx < (int)g.nx;
   for (uint32_t a0 = 0; a0 < cnt; a0 += kSrThreads) {
     const uint32_t ai = a0 + threadIdx.x;
     const bool active = ai < cnt;
     const double4 me = active ? pd[start + ai] : make_double4(0., 0., 0., 0.);
     double fx = 0.0, fy = 0.0, fz = 0.0, en = 0.0;
-    // (own cell first in the dx = 0 plane, as the reference's intra kernel)
-    for (int nbi = 0; nbi < 9 && plane_in; nbi++) {
-      const int o = (plane == 0) ? ((nbi + 4) % 9) : nbi;  // (0,0) first when dx = 0
-      const int dyc = o / 3 - 1, dzc = o % 3 - 1;
+    // (own cell first in its row, as the reference's intra kernel)
+    for (int nbi = 0; nbi < n && plane_in; nbi++) {
+      const int t = t0 + (own_row ? (nbi + n / 2) % n : nbi);
+      const int dyc = (t / 3) % 3 - 1, dzc = t % 3 - 1;
       const int jy = iy + dyc, jz = iz + dzc;
       if (jy < 0 || jz < 0 || jy >= (int)g.ny || jz >= (int)g.nz) continue;
-      const bool own = plane == 0 && dyc == 0 && dzc == 0;
+      const bool own = dx == 0 && dyc == 0 && dzc == 0;
       const uint32_t nb = (jx * g.ny + jy) * g.nz + jz;
       const uint32_t bcnt = cell_count[nb];
       const uint32_t bstart = cell_point[nb];
@@ -1195,8 +1209,8 @@ __device__ __forceinline__ void sr_block(const double4 *__restrict__ pd, const u
 __global__ void __launch_bounds__(kSrThreads)
 k_short_range(const double4 *__restrict__ pd, const uint32_t *__restrict__ cell_count,
               const uint32_t *__restrict__ cell_point, Grid g, uint32_t natom,
-              double4 *__restrict__ sr) {
-  sr_block(pd, cell_count, cell_point, g, natom, sr, blockIdx.x, blockIdx.y);
+              double4 *__restrict__ sr, uint32_t rows) {
+  sr_block(pd, cell_count, cell_point, g, natom, sr, rows, blockIdx.x, blockIdx.y);
 }
 
 // ----------------------------------------------------------------------------
@@ -1211,7 +1225,8 @@ constexpr int kCombineThreads = 256;
 constexpr int kCombineAtoms = 32;
 constexpr int kCombineWarps = kCombineThreads / 32;
 
-__device__ __forceinline__ void combine_block(const double4 *__restrict__ sr, const double4 *__restrict__ part,
+__device__ __forceinline__ void combine_block(const double4 *__restrict__ sr, uint32_t sr_rows,
+                                              const double4 *__restrict__ part,
                                               uint32_t nsplit, const uint32_t *__restrict__ sorted_idx,
                                               uint32_t natom, int use_far, double *__restrict__ cfx,
                                               double *__restrict__ cfy, double *__restrict__ cfz,
@@ -1241,7 +1256,7 @@ __device__ __forceinline__ void combine_block(const double4 *__restrict__ sr, co
       const double4 v = s_rows[k][lane];
       t.x += v.x; t.y += v.y; t.z += v.z; t.w += v.w;
     }
-    for (int pl = 0; pl < kSrPlanes; pl++) {
+    for (uint32_t pl = 0; pl < sr_rows; pl++) {
       const double4 v = sr[(size_t)pl * natom + p];
       t.x += v.x; t.y += v.y; t.z += v.z; t.w += v.w;
     }
@@ -1255,13 +1270,13 @@ __device__ __forceinline__ void combine_block(const double4 *__restrict__ sr, co
 }
 
 __global__ void __launch_bounds__(kCombineThreads)
-k_combine(const double4 *__restrict__ sr, const double4 *__restrict__ part, uint32_t nsplit,
+k_combine(const double4 *__restrict__ sr, uint32_t sr_rows, const double4 *__restrict__ part, uint32_t nsplit,
           const uint32_t *__restrict__ sorted_idx, uint32_t natom, int use_far,
           double *__restrict__ cfx, double *__restrict__ cfy, double *__restrict__ cfz,
           double *__restrict__ cen, double *__restrict__ ofx, double *__restrict__ ofy,
           double *__restrict__ ofz, double *__restrict__ oen, double *__restrict__ block_energy) {
-  combine_block(sr, part, nsplit, sorted_idx, natom, use_far, cfx, cfy, cfz, cen, ofx, ofy, ofz, oen, block_energy,
-                blockIdx.x);
+  combine_block(sr, sr_rows, part, nsplit, sorted_idx, natom, use_far, cfx, cfy, cfz, cen, ofx, ofy, ofz, oen,
+                block_energy, blockIdx.x);
 }
 
 // ----------------------------------------------------------------------------

@@ -48,7 +48,7 @@ constexpr size_t kOffSorted = kOffPerm + align256(4ull * kMaxAtoms);
 constexpr size_t kOffPk = kOffSorted + align256(4ull * kMaxAtoms);
 constexpr size_t kOffPd = kOffPk + align256(16ull * kMaxAtoms);
 constexpr size_t kOffSr = kOffPd + align256(32ull * kMaxAtoms);
-constexpr size_t kOffCellOut = kOffSr + align256(32ull * kdev::kSrPlanes * kMaxAtoms);
+constexpr size_t kOffCellOut = kOffSr + align256(32ull * kdev::kSrRowsPlanes * kMaxAtoms);
 constexpr size_t kOffBlockE = kOffCellOut + align256(4ull * 8ull * kMaxAtoms);
 constexpr size_t kScratchBytes =
     kOffBlockE + align256(8ull * ((kMaxAtoms + kdev::kCombineAtoms - 1) / kdev::kCombineAtoms));
@@ -185,10 +185,10 @@ extern "C" glst_status glst_near_field_noalloc(uint32_t natom, const double *d_r
     dev::k_scatter<<<nb, 256, 0, st>>>(atom_cell, atom_slot, cell_point, natom, perm);
     dev::k_sort_pack<<<(uint32_t)ncell, 256, dev::kSortCap * sizeof(uint32_t), st>>>(
         perm, cell_count, cell_point, g, atom_cell, natom, d_rx, d_ry, d_rz, d_qc, sorted, pk, pd);
-    dev::k_short_range<<<dim3((uint32_t)ncell, dev::kSrPlanes), dev::kSrThreads, 0, st>>>(
-        pd, cell_count, cell_point, g, natom, sr);
+    dev::k_short_range<<<dim3((uint32_t)ncell, dev::kSrRowsPlanes), dev::kSrThreads, 0, st>>>(
+        pd, cell_count, cell_point, g, natom, sr, dev::kSrRowsPlanes);
     dev::k_combine<<<(natom + dev::kCombineAtoms - 1) / dev::kCombineAtoms, dev::kCombineThreads, 0, st>>>(
-        sr, nullptr, 0, sorted, natom, 0, cell_out, cell_out + kMaxAtoms, cell_out + 2ull * kMaxAtoms,
+        sr, dev::kSrRowsPlanes, nullptr, 0, sorted, natom, 0, cell_out, cell_out + kMaxAtoms, cell_out + 2ull * kMaxAtoms,
         cell_out + 3ull * kMaxAtoms, d_fx, d_fy, d_fz, d_en, block_e);
     if ((e = cudaGetLastError()) != cudaSuccess) {
       std::snprintf(g_err, sizeof g_err, "kernel launch failed: %s", cudaGetErrorString(e));

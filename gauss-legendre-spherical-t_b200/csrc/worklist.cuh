@@ -16,7 +16,7 @@ namespace dev {
 
 struct SysDesc {
   Grid g;
-  uint32_t natom, combine_blocks, part_rows, use_far;
+  uint32_t natom, combine_blocks, part_rows, use_far, sr_rows;
   SatArgs sat;  // shell-sum arguments (S, node tables, nodes per CTA, row stride, R)
   const double *rx, *ry, *rz, *qc;
   uint32_t *atom_cell, *atom_slot, *perm, *sorted_idx, *cell_count, *cell_point;
@@ -127,14 +127,14 @@ __global__ void __launch_bounds__(kLrThreads, 7) k_long_range_multi(const SysDes
   }
 }
 
-// item (a, b) = (cell, neighbour plane)
+// item (a, b) = (cell, row of neighbour cells)
 __global__ void __launch_bounds__(kSrThreads) k_short_range_multi(const SysDesc *__restrict__ sys,
                                                                   const WorkItem *__restrict__ items,
                                                                   uint32_t n) {
   for (uint32_t it = blockIdx.x; it < n; it += gridDim.x) {
     const WorkItem w = items[it];
     const SysDesc &d = sys[w.sys];
-    sr_block(d.pd, d.cell_count, d.cell_point, d.g, d.natom, d.sr, w.a, w.b);
+    sr_block(d.pd, d.cell_count, d.cell_point, d.g, d.natom, d.sr, d.sr_rows, w.a, w.b);
     __syncthreads();
   }
 }
@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(kCombineThreads) k_combine_multi(const SysDesc
   for (uint32_t it = blockIdx.x; it < n; it += gridDim.x) {
     const WorkItem w = items[it];
     const SysDesc &d = sys[w.sys];
-    combine_block(d.sr, d.part, d.part_rows, d.sorted_idx, d.natom, d.use_far, d.cfx, d.cfy, d.cfz, d.cen, d.ofx,
+    combine_block(d.sr, d.sr_rows, d.part, d.part_rows, d.sorted_idx, d.natom, d.use_far, d.cfx, d.cfy, d.cfz, d.cen, d.ofx,
                   d.ofy, d.ofz, d.oen, d.block_energy, w.a);
     __syncthreads();
   }
