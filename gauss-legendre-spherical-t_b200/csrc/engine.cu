@@ -678,9 +678,18 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
               (force_global && force_global[0] == '1');
     h->sat_per_node = per_node;
     h->sat_budget = budget;
-    h->sat_nb = pow2_floor((uint32_t)std::max<size_t>(1, std::min<size_t>(8, budget / per_node)));
     GLST_TRY(set_kernel_attributes(h->device, smem_total));
     h->nsm = nsm;
+    // Nodes per CTA: the most (<= 32) with which four CTAs still share an
+    // SM, when that is 8 or more (4^3 cells: 32, 5^3: 16, 7^3: 8, as
+    // glst_autotune picks them; a 3,000-atom 4^3 solve 0.484 -> 0.421 ms
+    // against 8), else at most 8 within one CTA's shared memory.
+    const size_t xyz_used = h->sat_xyz ? xyz_bytes : 0;
+    const size_t four = h->smem_sm / 4 > xyz_used ? (h->smem_sm / 4 - xyz_used) / per_node : 0;
+    h->sat_nb = four >= 8 ? pow2_floor((uint32_t)std::min<size_t>(32, four))
+                          : pow2_floor((uint32_t)std::max<size_t>(1, std::min<size_t>(8, budget / per_node)));
+    // ... but no fewer than four CTAs per SM's worth of node blocks (few nodes)
+    while (h->sat_nb > 8 && (K + h->sat_nb - 1) / h->sat_nb < 4 * (size_t)nsm) h->sat_nb >>= 1;
     h->g_node_base = node_base;
     h->g_dir_base = dir_base;
     h->g_kappa_base = kappa_base;

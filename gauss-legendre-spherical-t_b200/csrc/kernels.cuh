@@ -9,7 +9,7 @@
 //              tiles, stored rounded to FP32)
 //   R[C][K]    float2: shell sum times weight times e^{+ik.c} (cell centre c)
 //   part[P][N] double4: long-range partial sums, one row per node chunk
-//   sr[N]      double4: near-field sums
+//   sr[W][N]   double4: near-field sums, one row per row of neighbour cells
 // Cell c = (ix*ny + iy)*nz + iz, as in the reference (src/glst_force.cu:379-382).
 #pragma once
 
