@@ -325,9 +325,11 @@ static constexpr size_t kMaxChunkNodes = 2048;
 static constexpr size_t kMinChunkNodes = 256;
 
 // Near-field rows (kernels.cuh): nine when three rows' CTAs (one per cell
-// and x plane) would be fewer than four per SM.
+// and x plane) would be fewer than six per SM (up to 6^3 cells on B200:
+// 13,500-18,000 atoms on 6^3 solve 2 % faster with nine; on 7^3 grids nine
+// rows gained nothing for 24,000 atoms and cost 0.2 % for 30,000).
 static uint32_t sr_rows_for(size_t ncell, int nsm) {
-  return 3 * ncell < 4 * (size_t)std::max(1, nsm) ? dev::kSrRowsLines : dev::kSrRowsPlanes;
+  return 3 * ncell < 6 * (size_t)std::max(1, nsm) ? dev::kSrRowsLines : dev::kSrRowsPlanes;
 }
 
 static uint32_t pow2_floor(uint32_t v) {

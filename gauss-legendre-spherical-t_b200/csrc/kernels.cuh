@@ -1146,9 +1146,9 @@ constexpr int kSrThreads = 128;
 // the row holding the cell itself starts with it.  Nine rows shorten each
 // thread's serial run of pairs threefold and triple the CTAs, for grids too
 // small to fill the GPU with three (3,000 atoms on 4^3 cells: 0.076 ->
-// 0.033 ms; 9,000 atoms on 5^3: 0.162 -> 0.092 ms); water10k's 7^3 grid
-// already has 1,029 CTAs, and there nine rows measured 0.2 % slower per
-// solve beside the far field.
+// 0.033 ms; 9,000 atoms on 5^3: 0.162 -> 0.092 ms; 18,000 on 6^3: 0.244 ->
+// 0.117 ms); water10k's 7^3 grid already has 1,029 CTAs, and there nine
+// rows measured 0.2 % slower per solve beside the far field.
 constexpr int kSrRowsPlanes = 3;
 constexpr int kSrRowsLines = 9;
 constexpr int kSrRowsMax = kSrRowsLines;
