@@ -373,3 +373,22 @@ def test_init_and_ncell_constructor(pkg, store):
     with pkg.GlstForce(len(x), tol, L, L, L, ncell=(4, 4, 4)) as g:
         assert tuple(g.info().ncell) == (4, 4, 4)
         assert g.info().cell_dim == L / 4
+
+
+def test_near_field_three_and_nine_rows(pkg, store):
+    """The near field's two launch forms against the oracle at 1e-12, on
+    grids with no far field (2 cells along x): 2 x 10 x 15 = 300 cells runs
+    three rows of 9 neighbour cells, 2 x 4 x 5 = 40 cells nine rows of 3."""
+    rng = np.random.default_rng(17)
+    for box, n in (((20.0, 100.0, 150.0), 6000), ((20.0, 40.0, 50.0), 1500)):
+        pts = rng.uniform(0.0, 1.0, size=(n, 3)) * np.asarray(box)
+        x, y, z = (np.ascontiguousarray(pts[:, i]) for i in range(3))
+        q = rng.choice([-0.5, 0.5], n)
+        f = pkg.GlstForce(n, 1e-5, *box, rcut=10.0)
+        f.calc_ener_force(*[_dev(a) for a in (x, y, z, q)])
+        got = f.get_ef()
+        assert f.info().has_far_field == 0
+        p = planner.make_plan(n, 1e-5, box, 10.0, store)
+        rep = oracle.error_report(got, oracle.glst(x, y, z, q, p))
+        assert rep["force_rms_rel"] <= 1e-12 and rep["energy_rel"] <= 1e-12, (box, rep)
+        f.close()

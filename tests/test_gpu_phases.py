@@ -210,3 +210,24 @@ def test_cells_beyond_the_shared_memory_sort(pkg):
     rep = oracle.error_report(got, oracle.coulomb(x, y, z, q))
     assert rep["force_rms_rel"] <= 1e-11, rep
     f.close()
+
+
+def test_sparse_outer_cell_layer(pkg, store):
+    """2,387 waters in a 41.5 A box at rcut 10 A: the reference's grid of
+    rcut-edged cells is 5^3 and its outer layer holds only the last 1.5 A of
+    the box (empty and near-empty cells), so 128-atom gather blocks span up
+    to 18 cell indices and up to 17 occupied cells (several staging passes
+    over the node tiles), and the near field runs in nine rows."""
+    from glst_b200 import systems
+    L, tol, rcut = 41.5, 1e-5, 10.0
+    x, y, z, q = systems.water_box(int(0.0334 * L ** 3), L, seed=21)
+    f, got = _solve(pkg, x, y, z, q, tol, (L, L, L), rcut)
+    p = planner.make_plan(len(x), tol, (L, L, L), rcut, store)
+    _ac, cnt, _pnt, _sidx = oracle.assign(x, y, z, p)
+    cnt = np.asarray(cnt)
+    cell_of_atom = np.repeat(np.arange(len(cnt)), cnt)
+    occupied = [len(np.unique(cell_of_atom[a0:a0 + 128])) for a0 in range(0, len(x), 128)]
+    assert tuple(f.info().ncell) == (5, 5, 5) and np.sum(cnt == 0) > 0 and max(occupied) > 8
+    rep = _check(f, got, oracle.glst(x, y, z, q, p), x, y, z, p)
+    print("sparse outer layer", rep)
+    f.close()
