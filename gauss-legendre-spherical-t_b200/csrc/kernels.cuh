@@ -941,7 +941,11 @@ struct LrChunk {
 // when they share a cell: 0.75 shared loads per (atom, node pair) instead of
 // 1.5) gave bitwise-equal results but ran 14 % slower (water10k 1.67 vs
 // 1.465 ms; 96 registers, 5 CTAs per SM): the MUFU latency the 32 resident
-// warps hide outweighs the MIO-queue relief.
+// warps hide outweighs the MIO-queue relief.  Staging the tiles with
+// asynchronous copies (cp.async, no prefetch registers: 64 registers without
+// spills) was bitwise-equal and slower too: 1.570 ms at 8 CTAs per SM, 1.584
+// at 9, 1.599 at 10 -- the copies add to the MIO queue, and more resident
+// warps do not help a gather bound by that queue.
 constexpr int kLrfCells = 4;           // cells staged per pass
 constexpr int kLrfTilePairs = 128;     // node pairs per cell tile
 constexpr int kLrfTileNodes = 2 * kLrfTilePairs;
