@@ -1175,10 +1175,17 @@ constexpr int kSrThreads = 128;
 // 0.033 ms; 9,000 atoms on 5^3: 0.162 -> 0.092 ms; 18,000 on 6^3: 0.244 ->
 // 0.117 ms); water10k's 7^3 grid already has 1,029 CTAs, and there nine
 // rows measured 0.2 % slower per solve beside the far field.
+// In the nine-row form each thread also runs two chains of accumulators
+// (pairs j and j+1) instead of one, so the FP64 pipe has more independent
+// work (3,000 atoms: near field 0.033 -> 0.025 ms, solve 0.141 -> 0.133 ms;
+// 9,000 atoms: solve 0.239 -> 0.223 ms).  The three-row form keeps one
+// chain: on water10k two chains made the near field 18 % faster alone but
+// the solve 0.2 % slower beside the far field.
 constexpr int kSrRowsPlanes = 3;
 constexpr int kSrRowsLines = 9;
 constexpr int kSrRowsMax = kSrRowsLines;
 
+template <bool kTwoChains>
 __device__ __forceinline__ void sr_block(const double4 *__restrict__ pd, const uint32_t *__restrict__ cell_count,
                                          const uint32_t *__restrict__ cell_point, const Grid &g, uint32_t natom,
                                          double4 *__restrict__ sr, uint32_t rows, uint32_t cell, uint32_t by) {
@@ -1213,18 +1220,51 @@ __device__ __forceinline__ void sr_block(const double4 *__restrict__ pd, const u
         if (threadIdx.x < nbt) s_at[threadIdx.x] = pd[bstart + b0 + threadIdx.x];
         __syncthreads();
         if (!active) continue;
-        for (uint32_t j = 0; j < nbt; j++) {
-          if (own && b0 + j == ai) continue;  // self
+        auto pair = [&](uint32_t j, double &ax, double &ay, double &az, double &an) {
+          if (own && b0 + j == ai) return;  // self
           const double4 o4 = s_at[j];
           const double dx = me.x - o4.x, dy = me.y - o4.y, dz = me.z - o4.z;
           const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
           const double ir = rsqrt(r2);
           const double e = me.w * o4.w * ir;
           const double fs = e * ir * ir;
-          fx = fma(fs, dx, fx);
-          fy = fma(fs, dy, fy);
-          fz = fma(fs, dz, fz);
-          en += e;
+          ax = fma(fs, dx, ax);
+          ay = fma(fs, dy, ay);
+          az = fma(fs, dz, az);
+          an += e;
+        };
+        if constexpr (kTwoChains) {
+          // branch-free pairs (the self pair selected to zero), so the two
+          // chains' instructions interleave
+          double gx = 0.0, gy = 0.0, gz = 0.0, gn = 0.0;
+          uint32_t j = 0;
+          for (; j + 1 < nbt; j += 2) {
+            const double4 o4 = s_at[j], p4 = s_at[j + 1];
+            const bool sa = own && b0 + j == ai, sb = own && b0 + j + 1 == ai;
+            const double dx = me.x - o4.x, dy = me.y - o4.y, dz = me.z - o4.z;
+            const double hx = me.x - p4.x, hy = me.y - p4.y, hz = me.z - p4.z;
+            const double r2 = sa ? 1.0 : fma(dx, dx, fma(dy, dy, dz * dz));
+            const double s2 = sb ? 1.0 : fma(hx, hx, fma(hy, hy, hz * hz));
+            const double ir = rsqrt(r2), is = rsqrt(s2);
+            const double e = sa ? 0.0 : me.w * o4.w * ir;
+            const double h = sb ? 0.0 : me.w * p4.w * is;
+            const double fs = e * ir * ir, hs = h * is * is;
+            fx = fma(fs, dx, fx);
+            gx = fma(hs, hx, gx);
+            fy = fma(fs, dy, fy);
+            gy = fma(hs, hy, gy);
+            fz = fma(fs, dz, fz);
+            gz = fma(hs, hz, gz);
+            en += e;
+            gn += h;
+          }
+          if (j < nbt) pair(j, fx, fy, fz, en);
+          fx += gx;
+          fy += gy;
+          fz += gz;
+          en += gn;
+        } else {
+          for (uint32_t j = 0; j < nbt; j++) pair(j, fx, fy, fz, en);
         }
       }
     }
@@ -1236,7 +1276,10 @@ __global__ void __launch_bounds__(kSrThreads)
 k_short_range(const double4 *__restrict__ pd, const uint32_t *__restrict__ cell_count,
               const uint32_t *__restrict__ cell_point, Grid g, uint32_t natom,
               double4 *__restrict__ sr, uint32_t rows) {
-  sr_block(pd, cell_count, cell_point, g, natom, sr, rows, blockIdx.x, blockIdx.y);
+  if (rows == kSrRowsLines)
+    sr_block<true>(pd, cell_count, cell_point, g, natom, sr, rows, blockIdx.x, blockIdx.y);
+  else
+    sr_block<false>(pd, cell_count, cell_point, g, natom, sr, rows, blockIdx.x, blockIdx.y);
 }
 
 // ----------------------------------------------------------------------------

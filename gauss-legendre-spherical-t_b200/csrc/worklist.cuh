@@ -134,7 +134,10 @@ __global__ void __launch_bounds__(kSrThreads) k_short_range_multi(const SysDesc 
   for (uint32_t it = blockIdx.x; it < n; it += gridDim.x) {
     const WorkItem w = items[it];
     const SysDesc &d = sys[w.sys];
-    sr_block(d.pd, d.cell_count, d.cell_point, d.g, d.natom, d.sr, d.sr_rows, w.a, w.b);
+    if (d.sr_rows == kSrRowsLines)
+      sr_block<true>(d.pd, d.cell_count, d.cell_point, d.g, d.natom, d.sr, d.sr_rows, w.a, w.b);
+    else
+      sr_block<false>(d.pd, d.cell_count, d.cell_point, d.g, d.natom, d.sr, d.sr_rows, w.a, w.b);
     __syncthreads();
   }
 }
