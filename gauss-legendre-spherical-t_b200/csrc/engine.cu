@@ -123,6 +123,8 @@ struct glst_handle {
   uint32_t sr_rows = dev::kSrRowsPlanes;  // near-field partial-sum rows
   size_t smem_sm = 0;  // shared memory per SM, less four CTAs' system reserve
   std::vector<uint32_t> g_node_base, g_dir_base, g_kappa_base;  // per group, internal order
+  std::vector<uint32_t> g_quad_base;  // per group, first radial-scale quad in kquads
+  dev::LrKappaQuads kquads{};         // the gather's radial scales (parameter space)
   uint32_t sat_nb = 1, sat_stride = 0;
   bool sat_xyz = true;  // shell-sum cell-coordinate table in shared memory
   uint32_t combine_blocks = 1;
@@ -455,6 +457,7 @@ static glst_status build_chunks(glst_handle *h, bool in_arena = false) {
         c.node_begin = dirs_all[i].k + j0 * g.n_radial - kb;
         c.dir_begin = h->g_dir_base[gi] + j_first + j0;
         c.kappa_begin = h->g_kappa_base[gi];
+        c.pad[0] = h->g_quad_base[gi];
         chunks.push_back(c);
       }
       // Structure-factor units: the group's whole run cut into units of
@@ -601,6 +604,9 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
   std::vector<uint32_t> radii(K);
   std::vector<float4> dirs;
   std::vector<float> kap;
+  std::vector<uint32_t> quad_base;  // per group, the first of its radial-scale quads
+  dev::LrKappaQuads kq{};
+  uint32_t nquad = 0;
   {
     uint32_t ref_base = 0, ibase = 0;
     for (size_t gi = 0; gi < (K ? p.groups.size() : 0); gi++) {
@@ -609,6 +615,14 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
       dir_base.push_back((uint32_t)dirs.size());
       node_base.push_back(ibase);
       for (unsigned r = 0; r < g.n_radial; r++) kap.push_back((float)g.kappa[r]);
+      quad_base.push_back(nquad);
+      for (unsigned r0 = 0; r0 < g.n_radial; r0 += 4, nquad++) {
+        if (nquad >= (uint32_t)dev::kLrKappaQuads)
+          return fail(GLST_ERR_SIZE, "more than %d radial-scale quads", dev::kLrKappaQuads);
+        float v[4];
+        for (unsigned i = 0; i < 4; i++) v[i] = r0 + i < g.n_radial ? (float)g.kappa[r0 + i] : 0.f;
+        kq.q[nquad] = make_float4(v[0], v[1], v[2], v[3]);
+      }
       for (unsigned j = 0; j < g.n_dir; j++)
         dirs.push_back(make_float4((float)g.dirs[3 * j], (float)g.dirs[3 * j + 1], (float)g.dirs[3 * j + 2], 0.f));
       for (unsigned j = 0; j < g.n_dir; j++) {
@@ -695,6 +709,8 @@ static glst_status setup(glst_handle *h, uint32_t natom, double tol,
     h->g_node_base = node_base;
     h->g_dir_base = dir_base;
     h->g_kappa_base = kappa_base;
+    h->g_quad_base = quad_base;
+    h->kquads = kq;
     {
       const Tuning t = tuned(p, h->K);
       if (t.sat_nb && !h->gsat)
@@ -840,7 +856,7 @@ static glst_status lr_stage(glst_handle *h, size_t stage, cudaStream_t st) {
     dev::k_long_range_flat<v><<<grid, dev::kLrThreads, 0, st>>>(h->pk, h->cell_point, h->plan.ncell,          \
                                                                 h->chunks + rg.c0, h->dirs, h->kappa, h->R,   \
                                                                 rg.kb, h->plan.natom, stage > 0 ? 1 : 0,      \
-                                                                h->part);                                     \
+                                                                h->part, h->kquads);                          \
     break;
   switch (h->lr_variant) {
     GLST_LR(0) GLST_LR(1) GLST_LR(2) GLST_LR(3)

@@ -972,14 +972,23 @@ __device__ __forceinline__ uint32_t cell_of_atom(const uint32_t *__restrict__ ce
   return lo;
 }
 
-template <uint32_t kPolyMask>
+// The radial scales of every group as quads (kappa_4t .. kappa_4t+3 of a
+// group, 0 beyond its last), passed in the gather's parameter space; a
+// chunk's quads start at quad_begin.
+constexpr int kLrKappaQuads = 128;
+struct LrKappaQuads {
+  float4 q[kLrKappaQuads];
+};
+
+template <uint32_t kPolyMask, bool kParamKappa>
 __device__ __forceinline__ void lr_block(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_point,
                                          uint32_t ncell, const LrChunk *__restrict__ chunks,
                                          const float4 *__restrict__ dirs, const float *__restrict__ kappa,
                                          const float2 *__restrict__ R, uint32_t node_off, uint32_t natom,
-                                         int accumulate, double4 *__restrict__ part, uint32_t bx, uint32_t by) {
+                                         int accumulate, double4 *__restrict__ part, uint32_t bx, uint32_t by,
+                                         const LrKappaQuads *kpq = nullptr) {
   __shared__ float4 s_n[2][kLrfCells * kLrfSlot];
-  __shared__ float4 s_kappa4[kLrfTilePairs / 2];
+  __shared__ float4 s_kappa4[kParamKappa ? 1 : kLrfTilePairs / 2];
   __shared__ uint32_t s_cells[kLrThreads];  // each thread's cell, then the distinct cells in order
   __shared__ uint32_t s_heads[kLrThreads / 32];
   const uint32_t a0 = bx * kLrThreads;
@@ -991,12 +1000,15 @@ __device__ __forceinline__ void lr_block(const float4 *__restrict__ pk, const ui
   const uint32_t dirs_per_tile = max(1u, (uint32_t)kLrfTilePairs / npr);  // npr <= kLrfTilePairs (host check)
   const uint32_t ntiles = (ch.n_dir + dirs_per_tile - 1) / dirs_per_tile;
   // radial scales of pairs (2t, 2t+1): kappa_{4t .. 4t+3}, 0 beyond the last
-  for (uint32_t t = threadIdx.x; 2 * t < npr; t += kLrThreads) {
-    float kq[4];
+  if constexpr (!kParamKappa) {
+    for (uint32_t t = threadIdx.x; 2 * t < npr; t += kLrThreads) {
+      float kq[4];
 #pragma unroll
-    for (int i = 0; i < 4; i++) kq[i] = 4 * t + i < nr ? kappa[ch.kappa_begin + 4 * t + i] : 0.f;
-    s_kappa4[t] = make_float4(kq[0], kq[1], kq[2], kq[3]);
+      for (int i = 0; i < 4; i++) kq[i] = 4 * t + i < nr ? kappa[ch.kappa_begin + 4 * t + i] : 0.f;
+      s_kappa4[t] = make_float4(kq[0], kq[1], kq[2], kq[3]);
+    }
   }
+  const float4 *kq4 = kParamKappa ? kpq->q + ch.pad[0] : s_kappa4;
   // The distinct cells of the CTA's atoms, in order, and each atom's rank
   // among them: windows of kLrfCells occupied cells.  (Windows of
   // consecutive cell indices made blocks that span empty and sparse cells --
@@ -1093,7 +1105,7 @@ __device__ __forceinline__ void lr_block(const float4 *__restrict__ pk, const ui
             float4 kq;
 #pragma unroll
             for (int q = 0; q < kLrGroup; q++) {
-              if ((q & 1) == 0) kq = s_kappa4[(k + q) >> 1];
+              if ((q & 1) == 0) kq = kq4[(k + q) >> 1];
               const float2 kp = (q & 1) ? make_float2(kq.z, kq.w) : make_float2(kq.x, kq.y);
               const float4 v = nn[k + q];
               if ((kPolyMask >> q) & 1u) {
@@ -1111,12 +1123,12 @@ __device__ __forceinline__ void lr_block(const float4 *__restrict__ pk, const ui
             }
           }
           for (; k + 2 <= npr; k += 2) {
-            const float4 kq = s_kappa4[k >> 1];
+            const float4 kq = kq4[k >> 1];
             sfu_pair(nn[k], make_float2(kq.x, kq.y));
             sfu_pair(nn[k + 1], make_float2(kq.z, kq.w));
           }
           if (k < npr) {
-            const float4 kq = s_kappa4[k >> 1];
+            const float4 kq = kq4[k >> 1];
             sfu_pair(nn[k], make_float2(kq.x, kq.y));
           }
           const float e = (EA.x + EA.y) - (EB.x + EB.y), gsum = G.x + G.y;
@@ -1152,9 +1164,10 @@ __global__ void __launch_bounds__(kLrThreads, 8)
 k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ cell_point, uint32_t ncell,
                   const LrChunk *__restrict__ chunks, const float4 *__restrict__ dirs,
                   const float *__restrict__ kappa, const float2 *__restrict__ R, uint32_t node_off,
-                  uint32_t natom, int accumulate, double4 *__restrict__ part) {
-  lr_block<kLrPolyMasks[kVariant]>(pk, cell_point, ncell, chunks, dirs, kappa, R, node_off, natom, accumulate,
-                                   part, blockIdx.x, blockIdx.y);
+                  uint32_t natom, int accumulate, double4 *__restrict__ part,
+                  const __grid_constant__ LrKappaQuads kpq) {
+  lr_block<kLrPolyMasks[kVariant], true>(pk, cell_point, ncell, chunks, dirs, kappa, R, node_off, natom,
+                                         accumulate, part, blockIdx.x, blockIdx.y, &kpq);
 }
 
 // ----------------------------------------------------------------------------

@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(kLrThreads, 7) k_long_range_multi(const SysDes
   for (uint32_t it = blockIdx.x; it < n; it += gridDim.x) {
     const WorkItem w = items[it];
     const SysDesc &d = sys[w.sys];
-    lr_block<kLrPolyMasks[0]>(d.pk, d.cell_point, d.g.ncell, d.chunks, d.dirs, d.kappa, d.R, 0, d.natom, 0,
+    lr_block<kLrPolyMasks[0], false>(d.pk, d.cell_point, d.g.ncell, d.chunks, d.dirs, d.kappa, d.R, 0, d.natom, 0,
                               d.part, w.a, w.b);
     __syncthreads();
   }
