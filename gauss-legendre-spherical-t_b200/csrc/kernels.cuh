@@ -1173,9 +1173,9 @@ k_long_range_flat(const float4 *__restrict__ pk, const uint32_t *__restrict__ ce
 // ----------------------------------------------------------------------------
 // Near field (src/glst_force.cu:1170-1544 restated): bare q_i q_j / r over
 // the own cell (self skipped) and the up to 26 neighbour cells inside the
-// grid (open boundary).  FP64 throughout.  CTA = (cell, neighbour plane
-// dx in {-1, 0, +1}); thread = atom; each plane writes its own partial row,
-// summed by k_combine in a fixed order.  Smaller CTAs (64 or 96 threads, which
+// grid (open boundary).  FP64 throughout.  CTA = (cell, row of neighbour
+// cells, below); thread = atom; each row writes its own partial row of
+// per-atom sums, summed by k_combine in a fixed order.  Smaller CTAs (64 or 96 threads, which
 // fit in the registers the shell-sum blocks leave free) measured slower on
 // water10k: 3.132 / 3.136 ms per solve against 3.122 ms.
 constexpr int kSrThreads = 128;
