@@ -945,7 +945,10 @@ struct LrChunk {
 // asynchronous copies (cp.async, no prefetch registers: 64 registers without
 // spills) was bitwise-equal and slower too: 1.570 ms at 8 CTAs per SM, 1.584
 // at 9, 1.599 at 10 -- the copies add to the MIO queue, and more resident
-// warps do not help a gather bound by that queue.
+// warps do not help a gather bound by that queue.  Reading each lane's R'
+// pair straight from global memory (two L1-cached loads per node pair, no
+// staging, barriers or window passes) was bitwise-equal and far slower:
+// 2.75 against 1.44 ms.
 constexpr int kLrfCells = 4;           // cells staged per pass
 constexpr int kLrfTilePairs = 128;     // node pairs per cell tile
 constexpr int kLrfTileNodes = 2 * kLrfTilePairs;
