@@ -411,6 +411,9 @@ __device__ __forceinline__ void sf_unit(const SfUnit &u, const float4 *__restric
     do {
       const uint32_t na = min((uint32_t)kSfAtomTile, cnt - a0);
       __syncthreads();
+      // (the atoms read from the staged tile, one broadcast shared load per
+      // atom per thread; broadcast global loads instead measured slower,
+      // water10k 1.133 against 1.088 ms, bitwise-equal)
       if (threadIdx.x < na) s_at[threadIdx.x] = pk[start + a0 + threadIdx.x];
       __syncthreads();
       // FR = sum q cos, FI = sum q sin (the sign of S's imaginary part is
