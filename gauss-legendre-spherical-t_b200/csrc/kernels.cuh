@@ -962,12 +962,13 @@ constexpr int kLrGroup = 14;      // node pairs per group (even: radial scales l
 static_assert(kLrGroup % 2 == 0, "groups are whole radial-scale quads");
 // Which pairs of a group take the FMA-pipe polynomial: bit q of the mask.
 // The variants are compiled in and chosen per plan by the autotuner
-// (glst_autotune); variant 0, three pairs in fourteen at 0, 5, 10, is the
+// (glst_autotune); variant 0, three pairs in fourteen at 1, 5, 10, is the
 // default.  With the radial scales in the parameter space (a lighter MIO
-// queue) three pairs beat two: water10k 1.406 ms at {0, 5, 10} against
-// 1.436 at {6, 13} (the earlier default); {2, 7, 12} 1.407, {4, 9, 13}
-// 1.410, {1, 6, 11} 1.419, four pairs {2, 6, 10, 13} 1.429.
-constexpr uint32_t kLrPolyMasks[4] = {(1u << 0) | (1u << 5) | (1u << 10), 0u, (1u << 6) | (1u << 13),
+// queue) three pairs beat two: water10k 1.397 ms at {1, 5, 10}, 1.406 at
+// {0, 5, 10}, against 1.436 at {6, 13} (the earlier default); {2, 7, 12}
+// 1.407, {4, 9, 13} 1.410, {0, 4, 9} 1.409, {1, 6, 11} 1.419, {0, 7} 1.420,
+// four pairs {2, 6, 10, 13} 1.429, {0, 4, 8, 12} 1.428.
+constexpr uint32_t kLrPolyMasks[4] = {(1u << 1) | (1u << 5) | (1u << 10), 0u, (1u << 6) | (1u << 13),
                                       (1u << 1) | (1u << 5) | (1u << 9) | (1u << 13)};
 constexpr int kLrVariants = 4;
 
