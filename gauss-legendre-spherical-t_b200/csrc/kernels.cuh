@@ -1134,6 +1134,12 @@ __device__ __forceinline__ void lr_block(const float4 *__restrict__ pk, const ui
               }
             }
           }
+          // The last, partial group of a direction stays on the SFU: its
+          // polynomial pairs, either guarded in a second unrolled copy of the
+          // group (water10k 1.491 ms) or one pair per step with a uniform
+          // test of the mask (1.511 ms), were slower than none (1.397 ms) --
+          // only interleaved with the SFU pairs of a full group does the
+          // polynomial's dependent chain hide.
           for (; k + 2 <= npr; k += 2) {
             const float4 kq = kq4[k >> 1];
             sfu_pair(nn[k], make_float2(kq.x, kq.y));
